@@ -1,0 +1,400 @@
+"""TEST ORACLE — not part of the product.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs import this module, and only
+as the checker or as the timed CPU baseline. It gives:
+
+* ``lib()``: the plain-C restatement ``magnet_oracle.c`` (ctypes), built by ``build()`` into oracle/_build/;
+* ``reference()``: the reference's own native module compiled from its sources by ``build_ref.sh`` into
+  oracle/_ref/ (present when the reference checkout was available at build time);
+* numpy restatements of the reference's Python drivers for the layout pass:
+  ``grid`` (magnet/tsne.py:30-46), ``kernel_spectra`` (magnet/tsne.py:48-71), ``optimize_tsne``
+  (magnet/tsne.py:132-214, the common fused path), ``sampling_frequencies`` / ``edge_schedule``
+  (magnet/__init__.py:51-66, 727-737) and ``optimize_sgd`` (MAGNET._optimize, magnet/__init__.py:751-839,
+  integer-epoch path);
+* ``fft_repulsion_fp64``: the FFT-interpolated repulsion with the reference's spread/gather and an FP64
+  convolution, and ``exact_repulsion``: the FP64 all-pairs sums.
+"""
+import ctypes
+import importlib.util
+import os
+import subprocess
+import sys
+import glob
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_BUILD = os.path.join(HERE, "_build")
+_LIB_PATH = os.path.join(_BUILD, "libmagnet_oracle.so")
+_REF_DIR = os.path.join(HERE, "_ref")
+
+_lib = None
+_ref = None
+
+
+def build(force=False):
+    """Compile the C restatement (gcc, IEEE single ops, no FMA contraction)."""
+    src = os.path.join(HERE, "magnet_oracle.c")
+    if not force and os.path.exists(_LIB_PATH) and os.path.getmtime(_LIB_PATH) >= os.path.getmtime(src):
+        return _LIB_PATH
+    os.makedirs(_BUILD, exist_ok=True)
+    tmp = _LIB_PATH + ".tmp"
+    subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c11", "-ffp-contract=off", "-fno-fast-math",
+                           src, "-o", tmp, "-lm"])
+    os.replace(tmp, _LIB_PATH)
+    return _LIB_PATH
+
+
+def build_reference():
+    """Compile the reference's native module from its sources (oracle/build_ref.sh); no-op when up to date or
+    when the sources are absent but a prebuilt module exists."""
+    subprocess.check_call(["bash", os.path.join(HERE, "build_ref.sh")])
+
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_F = ctypes.c_float
+
+
+class SgdArgs(ctypes.Structure):
+    _fields_ = [
+        ("Y", _P), ("n", _I64), ("dim", ctypes.c_int),
+        ("head", _P), ("tail", _P), ("eps", _P), ("eons", _P), ("eonns", _P), ("n_edges", _I64),
+        ("indptr", _P), ("indices", _P), ("walk_lens", _P), ("mid_pairs", _P), ("n_mid", ctypes.c_int),
+        ("jump_indptr", _P), ("jump_indices", _P), ("mid_jump", _F),
+        ("epoch_start", ctypes.c_int), ("epoch_end", ctypes.c_int), ("alpha0", _F), ("alpha1", _F),
+        ("mid_w0", _F), ("mid_w1", _F),
+        ("a", _F), ("b", _F), ("rep_a", _F), ("rep_b", _F), ("negative_sample_rate", _F), ("loss", ctypes.c_int),
+        ("exaggeration", _F), ("repulsion_strength", _F), ("walk_len", ctypes.c_int), ("mid_rate", _F),
+        ("optimizer", ctypes.c_int), ("clip_mode", ctypes.c_int), ("n_fixed", _I64),
+        ("adam_m", _P), ("adam_v", _P), ("adam_t", _P), ("beta1", _F), ("beta2", _F),
+        ("kernel", ctypes.c_int), ("node_b", _P), ("seed", ctypes.c_uint64),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_rng_stream.argtypes = [ctypes.c_uint64, _I64, _P]
+        L.orc_sgd_serial.argtypes = [ctypes.POINTER(SgdArgs), ctypes.c_int]
+        L.orc_sgd_serial.restype = ctypes.c_int
+        L.orc_sgd_schedule.argtypes = [ctypes.POINTER(SgdArgs), ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _I64, _P]
+        L.orc_sgd_schedule.restype = _I64
+        L.orc_spread.argtypes = [_P, _I64, _F, _F, _F, ctypes.c_int, ctypes.c_int, _P]
+        L.orc_gather.argtypes = [_P, _I64, _F, _F, _F, ctypes.c_int, ctypes.c_int, _P, _P]
+        L.orc_gather.restype = ctypes.c_double
+        L.orc_exact_repulsion.argtypes = [_P, _I64, _I64, _I64, ctypes.c_double, _P]
+        L.orc_exact_repulsion.restype = ctypes.c_double
+        L.orc_tsne_attraction.argtypes = [_P, _P, _P, _P, _I64, ctypes.c_int, _F, _P]
+        L.orc_tsne_step.argtypes = [_P, _P, _P, _P, _P, _I64, ctypes.c_int, _F, _F, _F, _F]
+        L.orc_bbox_2d.argtypes = [_P, _I64, _P]
+        _lib = L
+    return _lib
+
+
+def reference():
+    """The reference's compiled module (oracle/_ref/_magnet*.so), loaded under a private name so that it never
+    shadows a `_magnet` module of the product. None when it was not built."""
+    global _ref
+    if _ref is None:
+        cands = glob.glob(os.path.join(_REF_DIR, "_magnet*.so"))
+        if not cands:
+            return None
+        # a process that already imported the same file (e.g. as `_magnet` for the reference's Python package)
+        # must reuse it: initialising the extension twice registers its pybind11 types twice
+        for m in list(sys.modules.values()):
+            f = getattr(m, "__file__", None)
+            if f and os.path.realpath(f) == os.path.realpath(cands[0]):
+                _ref = m
+                return _ref
+        spec = importlib.util.spec_from_file_location("magnet_reference_native._magnet", cands[0])
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _ref = mod
+    return _ref
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _c32(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# ---------------------------------------------------------------------------------------------- RNG
+def rng_stream(seed, count):
+    out = np.empty(count, dtype=np.uint64)
+    lib().orc_rng_stream(ctypes.c_uint64(seed & (2 ** 64 - 1)), count, out.ctypes.data)
+    return out
+
+
+# ---------------------------------------------------------------------------------------------- SGD
+def _sgd_args(Y, head, tail, eps, eons, eonns, *, indptr=None, indices=None, walk_lens=None, mid_pairs=None,
+              jump_indptr=None, jump_indices=None, mid_jump=0.0, epoch_start=0, epoch_end=1, alpha0=1.0,
+              alpha1=1.0, mid_w0=0.0, mid_w1=0.0, a=1.577, b=0.895, rep_a=None, rep_b=1.0,
+              negative_sample_rate=5.0, loss=0, exaggeration=1.0, repulsion_strength=2.0, walk_len=4,
+              mid_rate=0.25, optimizer=0, clip_mode=0, n_fixed=0, adam_m=None, adam_v=None, adam_t=None,
+              beta1=0.9, beta2=0.999, kernel=0, node_b=None, seed=0, keep=None):
+    n, dim = Y.shape
+    if rep_a is None:
+        rep_a = a
+    args = SgdArgs()
+    args.Y = Y.ctypes.data; args.n = n; args.dim = dim
+    args.head = head.ctypes.data; args.tail = tail.ctypes.data; args.eps = eps.ctypes.data
+    args.eons = eons.ctypes.data; args.eonns = eonns.ctypes.data; args.n_edges = head.shape[0]
+    args.indptr = _ptr(indptr); args.indices = _ptr(indices); args.walk_lens = _ptr(walk_lens)
+    if mid_pairs is not None and mid_pairs.size > 0:
+        args.mid_pairs = mid_pairs.ctypes.data; args.n_mid = mid_pairs.shape[1]
+    else:
+        args.mid_pairs = None; args.n_mid = 0
+    if jump_indptr is not None and jump_indptr.size > 0:
+        args.jump_indptr = jump_indptr.ctypes.data; args.jump_indices = jump_indices.ctypes.data
+    args.mid_jump = mid_jump
+    args.epoch_start = epoch_start; args.epoch_end = epoch_end
+    args.alpha0 = alpha0; args.alpha1 = alpha1; args.mid_w0 = mid_w0; args.mid_w1 = mid_w1
+    args.a = a; args.b = b; args.rep_a = rep_a; args.rep_b = rep_b
+    args.negative_sample_rate = negative_sample_rate; args.loss = loss; args.exaggeration = exaggeration
+    args.repulsion_strength = repulsion_strength; args.walk_len = walk_len; args.mid_rate = mid_rate
+    args.optimizer = optimizer; args.clip_mode = clip_mode; args.n_fixed = n_fixed
+    args.adam_m = _ptr(adam_m); args.adam_v = _ptr(adam_v); args.adam_t = _ptr(adam_t)
+    args.beta1 = beta1; args.beta2 = beta2; args.kernel = kernel; args.node_b = _ptr(node_b)
+    args.seed = ctypes.c_uint64(seed & (2 ** 64 - 1)).value
+    return args
+
+
+def sgd_serial(Y, head, tail, eps, eons, eonns, per_edge_stream=False, **kw):
+    """optimize_layout at n_threads=1 (in place on Y, eons, eonns and the Adam state)."""
+    for a in (Y, eons, eonns):
+        assert a.flags.c_contiguous
+    args = _sgd_args(Y, head, tail, eps, eons, eonns, **kw)
+    lib().orc_sgd_serial(ctypes.byref(args), int(bool(per_edge_stream)))
+
+
+def sgd_schedule(Y, head, tail, eps, eons, eonns, epoch, per_edge_stream=False, negs_cap=None, **kw):
+    """Draws of one epoch: (sampled u8[E], n_neg i32[E], neg_off i64[E], negs i32[total], mid i32[E]).
+    eons / eonns are advanced in place."""
+    E = head.shape[0]
+    sampled = np.zeros(E, np.uint8); n_neg = np.zeros(E, np.int32); neg_off = np.zeros(E, np.int64)
+    mid = np.zeros(E, np.int32)
+    cap = negs_cap if negs_cap is not None else int(E * (float(kw.get("negative_sample_rate", 5.0)) + 2) + 64)
+    negs = np.zeros(cap, np.int32)
+    args = _sgd_args(Y, head, tail, eps, eons, eonns, **kw)
+    tot = lib().orc_sgd_schedule(ctypes.byref(args), int(epoch), int(bool(per_edge_stream)), sampled.ctypes.data,
+                                 n_neg.ctypes.data, neg_off.ctypes.data, negs.ctypes.data, cap, mid.ctypes.data)
+    assert tot <= cap, "negative buffer too small"
+    return sampled, n_neg, neg_off, negs[:tot], mid
+
+
+# ---------------------------------------------------------------------------------------------- t-SNE kernels
+def tsne_attraction(indptr, indices, data, Y, dof=1.0):
+    n, dim = Y.shape
+    out = np.empty_like(Y)
+    lib().orc_tsne_attraction(_c32(indptr, np.int32).ctypes.data, _c32(indices, np.int32).ctypes.data,
+                              _c32(data, np.float32).ctypes.data, Y.ctypes.data, n, dim, dof, out.ctypes.data)
+    return out
+
+
+def tsne_step(Y, U, G, A, F, rho, inv_sumQ, lr, momentum):
+    n, dim = Y.shape
+    lib().orc_tsne_step(Y.ctypes.data, U.ctypes.data, G.ctypes.data, _c32(A, np.float32).ctypes.data,
+                        _c32(F, np.float32).ctypes.data, n, dim, rho, inv_sumQ, lr, momentum)
+
+
+def bbox_2d(Y):
+    out = np.empty(4, np.float32)
+    lib().orc_bbox_2d(_c32(Y, np.float32).ctypes.data, Y.shape[0], out.ctypes.data)
+    return tuple(float(v) for v in out)
+
+
+# ---------------------------------------------------------------------------------------------- FFT repulsion
+def grid(Y, box_width=0.7, min_boxes=20, max_boxes=1000):
+    """FFTRepulsion2D._grid (magnet/tsne.py:30-46): (xmin, ymin, width, n_boxes)."""
+    xmin, ymin, xmax, ymax = bbox_2d(Y)
+    lo = np.array([xmin, ymin]) - 1e-3
+    hi = np.array([xmax, ymax]) + 1e-3
+    span = float((hi - lo).max())
+    n_boxes = int(np.clip(np.ceil(span / box_width), min_boxes, max_boxes))
+    n_boxes = min(max_boxes, -(-n_boxes // 4) * 4)
+    width = box_width if n_boxes * box_width >= span else max(span / n_boxes, 1e-12)
+    return float(lo[0]), float(lo[1]), width, n_boxes
+
+
+def kernel_spectra(n_boxes, width, n_interp=3, dof=1.0):
+    """FFTRepulsion2D._kernels (magnet/tsne.py:48-71) with the .real of __call__ (:86): (M, K1h, K2h)."""
+    import scipy.fft as fft
+    N = n_boxes * n_interp
+    M = fft.next_fast_len(2 * N, real=True)
+    delta = width / n_interp
+    off = np.arange(M)
+    off = np.where(off <= M // 2, off, off - M).astype(np.float64) * delta
+    r2 = off[:, None] ** 2 + off[None, :] ** 2
+    base = 1.0 + r2 / dof
+    K1 = (base ** (-dof)).astype(np.float32)
+    K2 = (base ** (-dof - 1.0)).astype(np.float32)
+    K1h = np.ascontiguousarray(fft.rfft2(K1), dtype=np.complex64)
+    K2h = np.ascontiguousarray(fft.rfft2(K2), dtype=np.complex64)
+    return int(M), np.ascontiguousarray(K1h.real), np.ascontiguousarray(K2h.real)
+
+
+def fft_repulsion_fp64(Y, xmin, ymin, width, n_boxes, n_interp=3, dof=1.0):
+    """The FFT-interpolated repulsion with the reference's box location and Lagrange weights, the spread and the
+    gather summed in FP64 and the grid convolution done exactly (FP64 FFT, zero padded). Returns (sumQ, F)."""
+    Y = _c32(Y, np.float32)
+    n = Y.shape[0]
+    N = n_boxes * n_interp
+    W = np.empty((3, N, N), np.float64)
+    lib().orc_spread(Y.ctypes.data, n, xmin, ymin, width, n_boxes, n_interp, W.ctypes.data)
+    M = 2 * N
+    delta = width / n_interp
+    off = np.arange(M)
+    off = np.where(off <= M // 2, off, off - M).astype(np.float64) * delta
+    r2 = off[:, None] ** 2 + off[None, :] ** 2
+    base = 1.0 + r2 / dof
+    K1h = np.fft.rfft2(base ** (-dof))
+    K2h = np.fft.rfft2(base ** (-dof - 1.0))
+    Wh = np.fft.rfft2(W, s=(M, M), axes=(1, 2))
+    phi = np.empty((4, N, N), np.float64)
+    phi[0] = np.fft.irfft2(K1h * Wh[0], s=(M, M))[:N, :N]
+    phi[1:] = np.fft.irfft2(K2h[None] * Wh, s=(M, M), axes=(1, 2))[:, :N, :N]
+    phi = np.ascontiguousarray(phi)
+    F = np.empty((n, 2), np.float64)
+    sumQ = lib().orc_gather(Y.ctypes.data, n, xmin, ymin, width, n_boxes, n_interp, phi.ctypes.data, F.ctypes.data)
+    return float(sumQ), F
+
+
+def exact_repulsion(Y, rows=None, dof=1.0):
+    """FP64 all-pairs (sumQ over the given rows, F of those rows)."""
+    Y = _c32(Y, np.float32)
+    n = Y.shape[0]
+    r0, r1 = (0, n) if rows is None else rows
+    F = np.empty((r1 - r0, 2), np.float64)
+    s = lib().orc_exact_repulsion(Y.ctypes.data, n, r0, r1, float(dof), F.ctypes.data)
+    return float(s), F
+
+
+# ---------------------------------------------------------------------------------------------- drivers
+def sampling_frequencies(w, target):
+    """magnet/__init__.py:51-66."""
+    w = np.asarray(w, dtype=np.float64)
+    n = len(w)
+    if n == 0 or n <= target:
+        return np.ones_like(w)
+    ws = np.sort(w)[::-1]
+    tail = np.cumsum(ws[::-1])[::-1]
+    t = np.arange(1, n + 1)
+    s_bp = 1.0 / np.maximum(ws[t - 1], 1e-300)
+    tail_t = np.append(tail[1:], 0.0)
+    total = t + s_bp * tail_t
+    k = int(np.searchsorted(total, target))
+    s = (target - k) / tail[k] if k < n and tail[k] > 0 else s_bp[-1]
+    return np.minimum(1.0, s * w)
+
+
+def edge_schedule(P, n_epochs, samples_per_node=5.0):
+    """magnet/__init__.py:727-737: (head, tail, epochs_per_sample) in COO order of the sorted CSR."""
+    C = P.tocoo()
+    w = C.data.astype(np.float64)
+    freq = sampling_frequencies(w, samples_per_node * P.shape[0])
+    budget = n_epochs if isinstance(n_epochs, (int, np.integer)) else 300
+    keep = freq >= 1.0 / budget
+    return (C.row[keep].astype(np.int32), C.col[keep].astype(np.int32), (1.0 / freq[keep]).astype(np.float32))
+
+
+def optimize_sgd(Y, head, tail, eps, n_epochs, *, lr=1.0, mid_weight=0.0, mid_phase=0.5, mid_pairs=None,
+                 backend="reference", n_threads=1, seed=0, a=1.577, b=0.895, rep_a=None, rep_b=1.0,
+                 negative_sample_rate=5.0, repulsion_strength=2.0, mid_rate=0.25, walk_len=4, n_fixed=0,
+                 indptr=None, indices=None, exaggeration=1.0):
+    """MAGNET._optimize, integer-epoch path with the default late_exaggeration = 1 (one segment
+    [0, n_epochs) with alpha and the mid weight interpolated linearly inside it; magnet/__init__.py:796-839).
+    backend: "reference" (the compiled reference, n_threads as given) or "oracle" (the C restatement)."""
+    n = Y.shape[0]
+    eons = eps.copy()
+    eonns = (eps / negative_sample_rate).astype(np.float32)
+    total = int(n_epochs)
+    mid_len = max(1.0, mid_phase * total)
+    use_mid = mid_weight > 0 and ((mid_pairs is not None and mid_pairs.size > 0) or walk_len > 0) and mid_rate > 0
+    alpha = lambda e: lr * (1.0 - e / total)
+    mid = (lambda e: mid_weight * max(0.0, 1.0 - e / mid_len)) if use_mid else (lambda e: 0.0)
+    if rep_a is None:
+        rep_a = a
+    mp = np.zeros((0, 1), np.int32) if mid_pairs is None else np.ascontiguousarray(mid_pairs, dtype=np.int32)
+    ip = np.zeros(0, np.int32) if indptr is None else np.ascontiguousarray(indptr, np.int32)
+    ix = np.zeros(0, np.int32) if indices is None else np.ascontiguousarray(indices, np.int32)
+    if backend == "reference":
+        R = reference()
+        z32 = np.zeros(0, np.int32)
+        R.optimize_layout(Y, head, tail, eps, eons, eonns, ip, ix, 0, total, float(alpha(0)), float(alpha(total)),
+                          float(mid(0)), float(mid(total)), float(a), float(b), float(rep_a), float(rep_b),
+                          float(negative_sample_rate), 0, float(exaggeration), float(repulsion_strength),
+                          int(walk_len), float(mid_rate), 0, 0, int(n_fixed),
+                          np.zeros((0, Y.shape[1]), np.float32), np.zeros((0, Y.shape[1]), np.float32), z32,
+                          0.9, 0.999, z32, mp, z32, z32, 0.0, 0, np.zeros(0, np.float32), int(seed), int(n_threads), 0)
+    else:
+        sgd_serial(Y, head, tail, eps, eons, eonns, indptr=ip if ip.size else None, indices=ix if ix.size else None,
+                   mid_pairs=mp if mp.size else None, epoch_start=0, epoch_end=total,
+                   alpha0=float(alpha(0)), alpha1=float(alpha(total)), mid_w0=float(mid(0)), mid_w1=float(mid(total)),
+                   a=a, b=b, rep_a=rep_a, rep_b=rep_b, negative_sample_rate=negative_sample_rate,
+                   exaggeration=exaggeration, repulsion_strength=repulsion_strength, walk_len=walk_len,
+                   mid_rate=mid_rate, n_fixed=n_fixed, seed=seed)
+    return Y
+
+
+def optimize_tsne(P, Y, n_iter=750, early_iter=250, early_exaggeration=12.0, exaggeration=1.0,
+                  learning_rate=None, momentum=(0.5, 0.8), n_interp=3, box_width=0.7, n_threads=-1,
+                  dof=1.0, backend="reference", callback=None):
+    """magnet/tsne.py:132-184 (the common path: no mid-range or far-field terms), driving the compiled
+    reference's kernels (backend "reference") or the C restatement with the FP64 convolution ("oracle")."""
+    import scipy.sparse as sp
+    n = P.shape[0]
+    P = sp.csr_matrix(P, dtype=np.float32)
+    P = P / P.sum()
+    indptr, indices, data = P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data.astype(np.float32)
+    if learning_rate is None:
+        learning_rate = max(200.0, n / early_exaggeration)
+    Y = np.ascontiguousarray(Y, dtype=np.float32)
+    update = np.zeros_like(Y)
+    gains = np.ones_like(Y)
+    R = reference() if backend == "reference" else None
+    convs, spectra = {}, {}
+    for it in range(n_iter):
+        early = it < early_iter
+        rho = early_exaggeration if early else exaggeration
+        mom = momentum[0] if early else momentum[1]
+        if R is not None:
+            attr = np.asarray(R.tsne_attraction(indptr, indices, data, Y, float(dof), n_threads))
+            xmin, ymin, xmax, ymax = R.bbox_2d(Y, n_threads)
+            lo = np.array([xmin, ymin]) - 1e-3
+            hi = np.array([xmax, ymax]) + 1e-3
+            span = float((hi - lo).max())
+            n_boxes = int(np.clip(np.ceil(span / box_width), 20, 1000))
+            n_boxes = min(1000, -(-n_boxes // 4) * 4)
+            width = box_width if n_boxes * box_width >= span else max(span / n_boxes, 1e-12)
+            key = (n_boxes, round(width, 6))
+            if key not in spectra:
+                if len(spectra) > 8:
+                    spectra.pop(next(iter(spectra)))
+                spectra[key] = kernel_spectra(n_boxes, width, n_interp, dof)
+            M, K1, K2 = spectra[key]
+            ck = (M, round(width, 6))
+            conv = convs.get(ck)
+            if conv is None:
+                conv = R.FFTConv2D(int(M), n_interp)
+                conv.set_kernels(K1, K2)
+                if len(convs) > 4:
+                    convs.pop(next(iter(convs)))
+                convs[ck] = conv
+            sumQ, F = conv.compute(Y, float(lo[0]), float(lo[1]), width, n_boxes, n_threads)
+            R.tsne_step(Y, update, gains, attr, np.asarray(F), float(rho), float(1.0 / max(sumQ, 1e-12)),
+                        float(learning_rate), float(mom), n_threads)
+        else:
+            attr = tsne_attraction(indptr, indices, data, Y, dof)
+            xmin, ymin, width, n_boxes = grid(Y, box_width)
+            sumQ, F = fft_repulsion_fp64(Y, xmin, ymin, width, n_boxes, n_interp, dof)
+            tsne_step(Y, update, gains, attr, F.astype(np.float32), float(rho), float(1.0 / max(sumQ, 1e-12)),
+                      float(learning_rate), float(mom))
+        if callback is not None:
+            callback(it, Y)
+    return Y
