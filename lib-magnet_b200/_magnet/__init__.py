@@ -1,0 +1,40 @@
+"""Drop-in replacement of the reference's native module `_magnet` (kerighan/lib-magnet, src/bindings.cpp).
+
+Put the directory holding this package ahead of the reference's extension on sys.path; the reference's Python
+package (`magnet`) then runs its layout pass on the B200: optimize_layout, FFTConv2D, tsne_attraction, tsne_step,
+tsne_update, bbox_2d and mid_spring come from the device library. The host-side kernels that stay on the
+reference's code (nn_descent, knn_search, smooth_knn, mid-near pairs, spectral init, louvain) are forwarded to
+the reference's own compiled module, found through the MAGNET_HOST_MODULE environment variable (path to the
+reference's `_magnet*.so`); without it they raise ImportError when used, as a missing `_magnet` would.
+"""
+import importlib.util as _ilu
+import os as _os
+
+from magnet_b200._native import (FFTConv2D, optimize_layout, tsne_attraction, tsne_step, tsne_update,  # noqa: F401
+                                 bbox_2d, mid_spring)
+
+_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search", "knn_search_sparse", "smooth_knn",
+               "mid_near_pairs_dense", "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration",
+               "louvain", "interp_scatter", "interp_gather", "scatter_padded_2d", "spectral_products",
+               "gather_forces_2d", "umap_attraction")
+
+
+def _load_host():
+    path = _os.environ.get("MAGNET_HOST_MODULE")
+    if not path:
+        return None
+    spec = _ilu.spec_from_file_location("magnet_host_native._magnet", path)
+    mod = _ilu.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_host = _load_host()
+
+
+def __getattr__(name):
+    if name in _HOST_NAMES:
+        if _host is None:
+            raise ImportError(f"_magnet.{name} runs on the reference's host module; set MAGNET_HOST_MODULE to its path")
+        return getattr(_host, name)
+    raise AttributeError(name)

@@ -1,0 +1,549 @@
+// C ABI of the layout pass (include/magnet_b200.h): argument checks with the reference's rules and messages,
+// staging of host arrays through per-thread device buffers, error codes with a thread-local message.
+#include "common.cuh"
+#include "fftrep.cuh"
+#include "fft.cuh"
+#include "tsne.cuh"
+#include "sgd.cuh"
+#include <string>
+#include <vector>
+#include <memory>
+#include <cstring>
+#include <cmath>
+#include <algorithm>
+#include <atomic>
+
+namespace mgb {
+
+namespace {
+thread_local std::string g_last_error;
+thread_local cudaStream_t g_stream = nullptr;
+
+// per-thread staging buffers (slots reused across calls)
+struct Stage {
+    DevBuf slot[24];
+    DevBuf scratch;
+};
+thread_local std::unique_ptr<Stage> g_stage;
+Stage& stage() {
+    if (!g_stage) g_stage.reset(new Stage());
+    return *g_stage;
+}
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return MG_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host out of memory";
+        return MG_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return MG_ERR_INTERNAL;
+    }
+}
+
+// device view of a caller array: the pointer itself when it is device memory, else a staged copy
+template <class T>
+T* in_dev(const T* p, int64_t count, int slot, cudaStream_t s) {
+    if (!p || count <= 0) return nullptr;
+    if (is_device_ptr(p)) return const_cast<T*>(p);
+    DevBuf& b = stage().slot[slot];
+    b.ensure(sizeof(T) * (size_t)count);
+    MGB_CUDA(cudaMemcpyAsync(b.p, p, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice, s));
+    return b.as<T>();
+}
+template <class T>
+T* out_dev(T* p, int64_t count, int slot) {
+    if (!p || count <= 0) return nullptr;
+    if (is_device_ptr(p)) return p;
+    DevBuf& b = stage().slot[slot];
+    b.ensure(sizeof(T) * (size_t)count);
+    return b.as<T>();
+}
+template <class T>
+void back(T* user, const T* dev, int64_t count, cudaStream_t s) {
+    if (!user || count <= 0 || user == dev) return;
+    MGB_CUDA(cudaMemcpyAsync(user, dev, sizeof(T) * (size_t)count, cudaMemcpyDeviceToHost, s));
+}
+bool any_host(std::initializer_list<const void*> ptrs) {
+    for (const void* p : ptrs)
+        if (p && !is_device_ptr(p)) return true;
+    return false;
+}
+
+// validate_csr of src/layout.hpp:21-32 (host arrays only; device arrays are the caller's responsibility)
+void validate_csr_host(const int32_t* ip, const int32_t* ix, int64_t nnz, int64_t n, int64_t n_cols,
+                       const char* what) {
+    if (!ip || is_device_ptr(ip)) return;
+    if (n_cols < 0) n_cols = n;
+    require(ip[0] == 0, std::string(what) + ": indptr[0] must be 0");
+    for (int64_t i = 0; i < n; ++i) require(ip[i + 1] >= ip[i], std::string(what) + ": indptr must be non-decreasing");
+    require((int64_t)ip[n] == nnz, std::string(what) + ": indices must have indptr[n] entries");
+    if (ix && !is_device_ptr(ix))
+        for (int64_t j = 0; j < nnz; ++j) require(ix[j] >= 0 && ix[j] < n_cols, "column index out of range");
+}
+
+__global__ void csr_sum_kernel(const float* __restrict__ P, int64_t nnz, double* __restrict__ out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int64_t e = threadIdx.x; e < nnz; e += blockDim.x) s += (double)P[e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        *out = t;
+    }
+}
+__global__ void csr_scale_kernel(const float* __restrict__ P, int64_t nnz, const double* __restrict__ sum,
+                                 float* __restrict__ out) {
+    const float s = (float)*sum;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = P[e] / s;
+}
+__global__ void read_sumq_kernel(const GridDesc* g, float* out) { *out = g->sumQ_f; }
+
+}  // namespace
+
+cudaStream_t current_stream() { return g_stream; }
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void count_launch(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+}  // namespace mgb
+
+using namespace mgb;
+
+// ============================================================================================== general
+extern "C" const char* mg_last_error(void) { return g_last_error.c_str(); }
+extern "C" int mg_version(void) { return 100; }
+extern "C" int mg_set_stream(void* stream) {
+    g_stream = static_cast<cudaStream_t>(stream);
+    return MG_OK;
+}
+extern "C" int mg_synchronize(void) {
+    return guard([&] { MGB_CUDA(cudaStreamSynchronize(current_stream())); });
+}
+extern "C" uint64_t mg_launch_count(void) { return launch_count(); }
+
+// ============================================================================================== FFTConv2D
+struct mg_fftconv {
+    int M = 0, ni = 3;
+    RepBuffers rb;
+    DevBuf gdesc;
+    bool kernels_set = false;
+};
+
+extern "C" int mg_fftconv_create(int M, int n_interp, mg_fftconv** out) {
+    return guard([&] {
+        require(out != nullptr, "out must not be NULL");
+        *out = nullptr;
+        require(M >= 2 && fft::is_5smooth(M), "M must be a 5-smooth FFT size >= 2 (2^a 3^b 5^c)");
+        require(M <= fft::kMaxLen, "M exceeds the supported maximum " + std::to_string(fft::kMaxLen));
+        require(n_interp >= 1 && n_interp <= 8, "n_interp must be between 1 and 8");
+        std::unique_ptr<mg_fftconv> h(new mg_fftconv());
+        h->M = M; h->ni = n_interp;
+        h->rb.alloc(M, M, n_interp);
+        h->gdesc.ensure(sizeof(GridDesc));
+        cudaStream_t s = current_stream();
+        MGB_CUDA(cudaMemsetAsync(h->gdesc.p, 0, sizeof(GridDesc), s));
+        rep_set_grid_host(h->gdesc.as<GridDesc>(), 0.f, 0.f, 1.f, 1, n_interp, M, s);
+        rep_twiddles(h->gdesc.as<GridDesc>(), h->rb, s, true);
+        MGB_CUDA(cudaStreamSynchronize(s));
+        *out = h.release();
+    });
+}
+
+extern "C" int mg_fftconv_set_kernels(mg_fftconv* h, const float* K1h, const float* K2h, int64_t rows, int64_t cols) {
+    return guard([&] {
+        require(h != nullptr, "null FFTConv2D handle");
+        const int Mh = h->M / 2 + 1;
+        require(rows == h->M && cols == Mh, "K1h must be (M, M/2+1) real");
+        require(K1h && K2h, "K1h must be (M, M/2+1) real");
+        cudaStream_t s = current_stream();
+        const int64_t cnt = rows * cols;
+        const float* d1 = in_dev(K1h, cnt, 0, s);
+        const float* d2 = in_dev(K2h, cnt, 1, s);
+        rep_set_spectra_from_host_layout(h->rb, d1, d2, h->M, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+        h->kernels_set = true;
+    });
+}
+
+extern "C" int mg_fftconv_compute(mg_fftconv* h, const float* Y, int64_t n, float xmin, float ymin, float width,
+                                  int n_boxes, float* sumQ, float* F) {
+    return guard([&] {
+        require(h != nullptr, "null FFTConv2D handle");
+        require(n >= 0, "Y must be (n, 2)");
+        const int64_t N = (int64_t)n_boxes * h->ni;
+        require(n_boxes >= 1 && N <= h->M && width > 0, "grid larger than the buffer");
+        require(h->kernels_set, "set_kernels must be called before compute");
+        require(sumQ != nullptr && (F != nullptr || n == 0), "sumQ and F must not be NULL");
+        cudaStream_t s = current_stream();
+        GridDesc* g = h->gdesc.as<GridDesc>();
+        rep_set_grid_host(g, xmin, ymin, width, n_boxes, h->ni, h->M, s);
+        const float2* Yd = reinterpret_cast<const float2*>(in_dev(Y, 2 * n, 2, s));
+        float2* Fd = reinterpret_cast<float2*>(out_dev(F, 2 * n, 3));
+        if (n > 0) rep_spread(Yd, n, g, h->rb, s);
+        rep_convolve(g, h->rb, n, s);
+        if (n > 0) rep_gather_forces(Yd, n, g, h->rb, Fd, s);
+        back(F, reinterpret_cast<float*>(Fd), 2 * n, s);
+        float* sq = out_dev(sumQ, 1, 4);
+        read_sumq_kernel<<<1, 1, 0, s>>>(g, sq);
+        MGB_LAUNCH_CHECK();
+        back(sumQ, sq, 1, s);
+        if (any_host({Y, F, sumQ})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" void mg_fftconv_destroy(mg_fftconv* h) { delete h; }
+
+// ============================================================================================== t-SNE kernels
+extern "C" int mg_tsne_attraction(const int32_t* indptr, const int32_t* indices, const float* data, int64_t nnz,
+                                  const float* Y, int64_t n, int dim, float dof, float* out) {
+    return guard([&] {
+        require(dof > 0.f, "dof must be positive");
+        require(dim >= 1 && dim <= kMaxDim, "dim out of range");
+        require(n >= 0 && indptr != nullptr, "indptr must have n + 1 entries");
+        validate_csr_host(indptr, indices, nnz, n, -1, "tsne_attraction");
+        cudaStream_t s = current_stream();
+        const int32_t* ip = in_dev(indptr, n + 1, 0, s);
+        const int32_t* ix = in_dev(indices, nnz, 1, s);
+        const float* P = in_dev(data, nnz, 2, s);
+        const float* Yd = in_dev(Y, n * dim, 3, s);
+        float* od = out_dev(out, n * dim, 4);
+        tsne_attraction_dev(ip, ix, P, Yd, n, dim, dof, od, s);
+        back(out, od, n * dim, s);
+        if (any_host({indptr, indices, data, Y, out})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+static int step_impl(float* Y, float* update, float* gains, const float* A, const float* F, int64_t n, int dim,
+                     float rho, float inv_sumQ, float lr, float momentum, bool fused) {
+    return guard([&] {
+        require(dim >= 1 && dim <= kMaxDim && n >= 1, "Y must be 2-d");
+        require(Y && update && gains && A && (F || !fused), "arrays must match Y");
+        cudaStream_t s = current_stream();
+        const int64_t t = n * dim;
+        float* Yd = in_dev(Y, t, 0, s);
+        float* Ud = in_dev(update, t, 1, s);
+        float* Gd = in_dev(gains, t, 2, s);
+        const float* Ad = in_dev(A, t, 3, s);
+        const float* Fd = fused ? in_dev(F, t, 4, s) : nullptr;
+        if (fused) tsne_step_dev(Yd, Ud, Gd, Ad, Fd, n, dim, rho, inv_sumQ, lr, momentum, stage().scratch, s);
+        else tsne_update_dev(Yd, Ud, Gd, Ad, n, dim, lr, momentum, stage().scratch, s);
+        back(Y, Yd, t, s); back(update, Ud, t, s); back(gains, Gd, t, s);
+        if (any_host({Y, update, gains, A, F})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" int mg_tsne_step(float* Y, float* update, float* gains, const float* attr, const float* F, int64_t n,
+                            int dim, float rho, float inv_sumQ, float lr, float momentum) {
+    return step_impl(Y, update, gains, attr, F, n, dim, rho, inv_sumQ, lr, momentum, true);
+}
+
+extern "C" int mg_tsne_update(float* Y, float* update, float* gains, const float* grad, int64_t n, int dim, float lr,
+                              float momentum) {
+    return step_impl(Y, update, gains, grad, nullptr, n, dim, 0.f, 0.f, lr, momentum, false);
+}
+
+extern "C" int mg_bbox_2d(const float* Y, int64_t n, float* out4) {
+    return guard([&] {
+        require(n >= 1 && Y && out4, "Y must be (n, 2)");
+        cudaStream_t s = current_stream();
+        const float* Yd = in_dev(Y, 2 * n, 0, s);
+        float* od = out_dev(out4, 4, 1);
+        bbox_dev(Yd, n, od, stage().scratch, s);
+        back(out4, od, 4, s);
+        if (any_host({Y, out4})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" int mg_mid_spring(const float* Y, const int32_t* pairs, float* grad, int64_t n, int dim, int m, float w) {
+    return guard([&] {
+        require(Y && pairs && grad && n >= 0 && dim >= 1 && dim <= kMaxDim && m >= 1, "bad shapes");
+        cudaStream_t s = current_stream();
+        const float* Yd = in_dev(Y, n * dim, 0, s);
+        const int32_t* pd = in_dev(pairs, n * m, 1, s);
+        float* gd = in_dev(grad, n * dim, 2, s);
+        mid_spring_dev(Yd, pd, gd, n, dim, m, w, s);
+        back(grad, gd, n * dim, s);
+        if (any_host({Y, pairs, grad})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+// ============================================================================================== t-SNE loop
+extern "C" void mg_tsne_params_default(mg_tsne_params* p) {
+    if (!p) return;
+    p->n_iter = 750; p->early_iter = 250; p->early_exaggeration = 12.f; p->exaggeration = 1.f;
+    p->learning_rate = -1.f; p->momentum_early = 0.5f; p->momentum_late = 0.8f; p->n_interp = 3;
+    p->box_width = 0.7f; p->min_boxes = 20; p->max_boxes = 1000; p->dof = 1.f; p->threads_per_row = 0;
+    p->use_graph = 1;
+}
+
+namespace mgb {
+// shared by the C ABI and the batch / serving layers
+void tsne_prepare(TsneDev& d, const int32_t* indptr, const int32_t* indices, const float* P, int64_t n, int64_t nnz,
+                  const mg_tsne_params& p, double box_width_exact, cudaStream_t s) {
+    require(n >= 1, "the layout needs at least one point");
+    require(p.n_iter >= 0 && p.early_iter >= 0, "iteration counts must be non-negative");
+    require(p.dof > 0.f, "dof must be positive");
+    require(p.box_width > 0.f, "box_width must be positive");
+    validate_csr_host(indptr, indices, nnz, n, -1, "optimize_tsne");
+    TsneSched sc{};
+    sc.early_iter = p.early_iter; sc.early_exag = p.early_exaggeration; sc.exag = p.exaggeration;
+    sc.mom0 = p.momentum_early; sc.mom1 = p.momentum_late;
+    const double lr = p.learning_rate > 0.f ? (double)p.learning_rate
+                                            : std::max(200.0, (double)n / (double)p.early_exaggeration);
+    sc.lr = (float)lr;
+    sc.inv_dof = 1.f / p.dof;
+    sc.box_width = box_width_exact > 0 ? box_width_exact : (double)p.box_width;
+    sc.min_boxes = p.min_boxes; sc.max_boxes = p.max_boxes; sc.ni = p.n_interp;
+    const int32_t* ip = in_dev(indptr, n + 1, 0, s);
+    const int32_t* ix = in_dev(indices, nnz, 1, s);
+    const float* Pd = in_dev(P, nnz, 2, s);
+    d.init(ip, ix, Pd, n, nnz, false, sc, p.dof, p.threads_per_row, s);
+    // P / P.sum() (magnet/tsne.py:149-150)
+    if (nnz > 0) {
+        double* sum = static_cast<double*>(stage().scratch.ensure(sizeof(double)));
+        csr_sum_kernel<<<1, 1024, 0, s>>>(d.P.as<float>(), nnz, sum);
+        MGB_LAUNCH_CHECK();
+        csr_scale_kernel<<<256, 256, 0, s>>>(d.P.as<float>(), nnz, sum, d.P.as<float>());
+        MGB_LAUNCH_CHECK();
+    }
+}
+}  // namespace mgb
+
+namespace {
+// the device state of the calling thread's last t-SNE pass: buffers and the captured iteration are reused by the
+// next call with the same sizes (the reference keeps its FFTConv2D objects for the same reason)
+thread_local std::unique_ptr<TsneDev> g_tsne;
+TsneDev& tsne_state() {
+    if (!g_tsne) g_tsne.reset(new TsneDev());
+    return *g_tsne;
+}
+}  // namespace
+
+static void optimize_tsne_impl(const int32_t* indptr, const int32_t* indices, const float* P, int64_t n, int64_t nnz,
+                               float* Y, const mg_tsne_params* p, double* stage_ms, int* grid) {
+    mg_tsne_params def;
+    mg_tsne_params_default(&def);
+    const mg_tsne_params& pp = p ? *p : def;
+    require(Y != nullptr, "Y must be (n, 2)");
+    cudaStream_t s = current_stream();
+    TsneDev& d = tsne_state();
+    tsne_prepare(d, indptr, indices, P, n, nnz, pp, (double)pp.box_width, s);
+    const float* Yd = in_dev(Y, 2 * n, 3, s);
+    d.set_layout(Yd, false, s);
+    if (stage_ms) d.run_profiled(pp.n_iter, s, stage_ms, grid);
+    else d.run(pp.n_iter, pp.use_graph != 0, s);
+    d.get_layout(Y, !is_device_ptr(Y), s);
+}
+
+extern "C" int mg_optimize_tsne(const int32_t* indptr, const int32_t* indices, const float* P, int64_t n, int64_t nnz,
+                                float* Y, const mg_tsne_params* p) {
+    return guard([&] { optimize_tsne_impl(indptr, indices, P, n, nnz, Y, p, nullptr, nullptr); });
+}
+
+extern "C" int mg_optimize_tsne_profiled(const int32_t* indptr, const int32_t* indices, const float* P, int64_t n,
+                                         int64_t nnz, float* Y, const mg_tsne_params* p, double* stage_ms, int* grid) {
+    return guard([&] {
+        require(stage_ms != nullptr, "stage_ms must hold 9 values");
+        for (int k = 0; k < 9; ++k) stage_ms[k] = 0.0;
+        optimize_tsne_impl(indptr, indices, P, n, nnz, Y, p, stage_ms, grid);
+        MGB_CUDA(cudaStreamSynchronize(current_stream()));
+    });
+}
+
+extern "C" int mg_center_scale(float* Y, int64_t n, int dim, double target_std) {
+    return guard([&] {
+        require(Y && n >= 1 && dim >= 1 && dim <= kMaxDim, "Y must be (n, dim)");
+        cudaStream_t s = current_stream();
+        float* Yd = in_dev(Y, n * dim, 0, s);
+        center_scale_dev(Yd, n, dim, target_std, stage().scratch, s);
+        back(Y, Yd, n * dim, s);
+        if (!is_device_ptr(Y)) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+// ============================================================================================== SGD
+extern "C" void mg_layout_args_default(mg_layout_args* a) {
+    if (!a) return;
+    std::memset(a, 0, sizeof(*a));
+    a->alpha0 = 1.f; a->alpha1 = 1.f; a->a = 1.577f; a->b = 0.895f; a->rep_a = 1.577f; a->rep_b = 1.f;
+    a->negative_sample_rate = 5.f; a->exaggeration = 1.f; a->repulsion_strength = 2.f; a->walk_len = 4;
+    a->mid_rate = 0.25f; a->beta1 = 0.9f; a->beta2 = 0.999f; a->n_threads = -1;
+}
+
+namespace {
+
+// the reference's checks (src/layout.cpp:360-437) and derived scalars; stages the arrays
+SgdDev prepare_sgd(const mg_layout_args& A, cudaStream_t s) {
+    require(A.Y != nullptr && A.n >= 0, "Y must be 2-dimensional");
+    const int64_t n = A.n;
+    const int dim = A.dim;
+    require(dim >= 1 && dim <= kMaxDim, "n_components must be between 1 and 64");
+    const int64_t E = A.n_edges;
+    require(E >= 0, "head must be 1-d");
+    require(E == 0 || (A.head && A.tail && A.epochs_per_sample && A.epoch_of_next_sample && A.epoch_of_next_negative_sample),
+            "head, tail and epoch arrays must have the same length");
+    require(A.epoch_start >= 0 && A.epoch_end >= A.epoch_start, "invalid epoch range");
+    require(A.negative_sample_rate > 0.0f, "negative_sample_rate must be positive");
+    require(A.loss == 0 || A.loss == 1, "loss must be 0 (umap) or 1 (infonce)");
+    require(A.kernel >= 0 && A.kernel <= 3, "kernel must be 0 (power), 1 (gaussian), 2 (sech) or 3 (tanh)");
+    require(A.loss == 0 || A.kernel == 0, "the InfoNCE loss supports the power kernel only");
+    require(A.parallel == 0 || A.parallel == 1, "parallel must be 0 (hogwild) or 1 (owner)");
+    require(A.parallel == 0 || A.loss == 0, "parallel='owner' supports the umap loss only (InfoNCE moves the negatives)");
+    if (A.parallel == 1) throw Error(MG_ERR_NOT_SUPPORTED, "parallel='owner' is not available on the device path");
+    require(A.n_fixed >= 0 && A.n_fixed <= n, "n_fixed out of range");
+    require(A.stream_mode == 0 || A.stream_mode == 1, "stream_mode must be 0 (per-edge streams) or 1 (serial stream)");
+    if (A.stream_mode == 1 && A.optimizer == 1)
+        throw Error(MG_ERR_NOT_SUPPORTED, "the serial stream mode supports the sgd optimizer only");
+    if (A.head && !is_device_ptr(A.head)) {
+        for (int64_t i = 0; i < E; ++i) {
+            require(A.head[i] >= 0 && A.head[i] < n && A.tail[i] >= 0 && A.tail[i] < n, "edge index out of range");
+            require(A.epochs_per_sample[i] > 0.0f, "epochs_per_sample must be positive");
+        }
+    }
+    const bool adam = A.optimizer == 1;
+    if (adam) require(A.adam_m && A.adam_v && A.adam_t, "Adam state arrays have the wrong shape");
+    const bool has_pairs = A.mid_pairs != nullptr && A.n_mid > 0;
+    if (has_pairs && !is_device_ptr(A.mid_pairs))
+        for (int64_t i = 0; i < n * A.n_mid; ++i)
+            require(A.mid_pairs[i] >= 0 && A.mid_pairs[i] < n, "mid_pairs index out of range");
+    const bool has_jumps = A.jump_indptr != nullptr && A.mid_jump > 0.0f;
+    if (has_jumps) validate_csr_host(A.jump_indptr, A.jump_indices, A.jump_nnz, n, -1, "jump graph");
+    const bool walks = has_jumps || !has_pairs;
+    const bool use_mid = (A.mid_w0 > 0.0f || A.mid_w1 > 0.0f) && A.mid_rate > 0.0f && (has_pairs || A.walk_len > 0);
+    if (use_mid && walks) {
+        require(A.indptr != nullptr, "indptr must have n + 1 entries");
+        validate_csr_host(A.indptr, A.indices, A.graph_nnz, n, -1, "graph");
+    }
+    if (use_mid && A.walk_lens && !is_device_ptr(A.walk_lens))
+        for (int64_t i = 0; i < n; ++i) require(A.walk_lens[i] >= 0 && A.walk_lens[i] <= 64, "walk_lens out of range");
+    float rep_a = A.rep_a, rep_b = A.rep_b;
+    const bool rep_coupled = rep_b <= 0.0f;
+    if (rep_b <= 0.0f) { rep_a = A.a; rep_b = A.b; }
+    require(rep_a > 0.0f, "repulsion kernel a must be positive");
+    if (A.node_b && !is_device_ptr(A.node_b))
+        for (int64_t i = 0; i < n; ++i) require(A.node_b[i] > 0.05f && A.node_b[i] <= 2.0f, "node_b out of range");
+
+    SgdDev c{};
+    c.n = n; c.dim = dim; c.n_edges = E;
+    c.Y = in_dev(A.Y, n * dim, 0, s);
+    c.head = in_dev(A.head, E, 1, s);
+    c.tail = in_dev(A.tail, E, 2, s);
+    c.eps = in_dev(A.epochs_per_sample, E, 3, s);
+    c.eons = in_dev(A.epoch_of_next_sample, E, 4, s);
+    c.eonns = in_dev(A.epoch_of_next_negative_sample, E, 5, s);
+    c.mid_pairs = has_pairs && !has_jumps ? in_dev(A.mid_pairs, n * A.n_mid, 6, s) : nullptr;
+    c.n_mid = has_pairs ? A.n_mid : 0;
+    c.jump_indptr = has_jumps ? in_dev(A.jump_indptr, n + 1, 7, s) : nullptr;
+    c.jump_indices = has_jumps ? in_dev(A.jump_indices, A.jump_nnz, 8, s) : nullptr;
+    c.mid_jump = A.mid_jump;
+    c.indptr = (use_mid && walks) ? in_dev(A.indptr, n + 1, 9, s) : nullptr;
+    c.indices = (use_mid && walks) ? in_dev(A.indices, A.graph_nnz, 10, s) : nullptr;
+    c.walk_lens = (use_mid && A.walk_lens) ? in_dev(A.walk_lens, n, 11, s) : nullptr;
+    c.node_b = A.node_b ? in_dev(A.node_b, n, 12, s) : nullptr;
+    if (adam) {
+        c.adam_m = in_dev(A.adam_m, n * dim, 13, s);
+        c.adam_v = in_dev(A.adam_v, n * dim, 14, s);
+        c.adam_t = in_dev(A.adam_t, n, 15, s);
+    }
+    c.beta1 = A.beta1; c.beta2 = A.beta2;
+    c.a = A.a; c.b = A.b; c.rep_a = rep_a; c.rep_b = rep_b;
+    c.two_ab = 2.0f * A.a * A.b;
+    c.two_b = 2.0f * rep_b * A.repulsion_strength;
+    c.negative_sample_rate = A.negative_sample_rate; c.exaggeration = A.exaggeration;
+    c.repulsion_strength = A.repulsion_strength; c.mid_rate = A.mid_rate;
+    c.b_is_one = std::fabs(A.b - 1.0f) < 1e-6f;
+    c.rep_b_is_one = std::fabs(rep_b - 1.0f) < 1e-6f;
+    c.rep_coupled = rep_coupled;
+    c.use_mid = use_mid;
+    c.m_neg = (int)std::min<long>(64, std::max<long>(1, std::lround(A.negative_sample_rate)));
+    c.walk_len = A.walk_len; c.loss = A.loss; c.clip_mode = A.clip_mode; c.kernel = A.kernel;
+    c.optimizer = A.optimizer; c.n_fixed = A.n_fixed; c.seed = A.seed;
+    return c;
+}
+
+void sgd_copy_back(const mg_layout_args& A, const SgdDev& c, cudaStream_t s) {
+    back(A.Y, c.Y, c.n * c.dim, s);
+    back(A.epoch_of_next_sample, c.eons, c.n_edges, s);
+    back(A.epoch_of_next_negative_sample, c.eonns, c.n_edges, s);
+    if (A.optimizer == 1) {
+        back(A.adam_m, c.adam_m, c.n * c.dim, s);
+        back(A.adam_v, c.adam_v, c.n * c.dim, s);
+        back(A.adam_t, c.adam_t, c.n, s);
+    }
+}
+
+thread_local std::unique_ptr<SgdWork> g_sgd_work;
+
+}  // namespace
+
+extern "C" int mg_optimize_layout(const mg_layout_args* a) {
+    return guard([&] {
+        require(a != nullptr, "args must not be NULL");
+        cudaStream_t s = current_stream();
+        SgdDev c = prepare_sgd(*a, s);
+        if (!g_sgd_work) g_sgd_work.reset(new SgdWork());
+        if (c.n_edges > 0 && a->epoch_end > a->epoch_start)
+            sgd_run(c, *g_sgd_work, a->stream_mode, a->epoch_start, a->epoch_end, a->alpha0, a->alpha1, a->mid_w0,
+                    a->mid_w1, s);
+        sgd_copy_back(*a, c, s);
+        if (any_host({a->Y, a->epoch_of_next_sample, a->epoch_of_next_negative_sample, a->adam_m}))
+            MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* sampled, int32_t* n_neg,
+                                  int64_t* neg_off, int32_t* negs, int64_t negs_cap, int64_t* n_negs, int32_t* mid) {
+    return guard([&] {
+        require(a != nullptr, "args must not be NULL");
+        require(sampled && n_neg && neg_off && mid && n_negs, "outputs must not be NULL");
+        require(epoch >= a->epoch_start && epoch < std::max(a->epoch_end, a->epoch_start + 1), "epoch outside the call's range");
+        cudaStream_t s = current_stream();
+        SgdDev c = prepare_sgd(*a, s);
+        if (!g_sgd_work) g_sgd_work.reset(new SgdWork());
+        const int64_t E = c.n_edges;
+        float alpha, mid_w;
+        sgd_sched(c, epoch, a->epoch_start, a->epoch_end, a->alpha0, a->alpha1, a->mid_w0, a->mid_w1, alpha, mid_w);
+        int32_t* cnt_d = out_dev(n_neg, E, 16);
+        int64_t* off_d = out_dev(neg_off, E, 17);
+        int32_t* negs_d = out_dev(negs, std::max<int64_t>(negs_cap, 1), 18);
+        int32_t* mid_d = out_dev(mid, E, 19);
+        int64_t* tot_d = out_dev(n_negs, 1, 20);
+        sgd_record(c, *g_sgd_work, a->stream_mode, epoch, alpha, mid_w, cnt_d, off_d, negs_d, negs_cap, mid_d, tot_d, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> cnt_h(E);
+        if (E > 0) MGB_CUDA(cudaMemcpy(cnt_h.data(), cnt_d, sizeof(int32_t) * E, cudaMemcpyDeviceToHost));
+        back(neg_off, off_d, E, s);
+        back(mid, mid_d, E, s);
+        back(n_negs, tot_d, 1, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+        int64_t tot = 0;
+        if (is_device_ptr(n_negs)) MGB_CUDA(cudaMemcpy(&tot, n_negs, sizeof(int64_t), cudaMemcpyDeviceToHost));
+        else tot = *n_negs;
+        if (negs && negs_cap > 0) back(negs, negs_d, std::min(tot, negs_cap), s);
+        // sampled flags and n_neg in the reference's recording convention (0 when not sampled)
+        std::vector<uint8_t> sm(E);
+        for (int64_t i = 0; i < E; ++i) { sm[i] = cnt_h[i] >= 0; cnt_h[i] = std::max(cnt_h[i], 0); }
+        if (is_device_ptr(sampled)) MGB_CUDA(cudaMemcpy(sampled, sm.data(), E, cudaMemcpyHostToDevice));
+        else std::memcpy(sampled, sm.data(), E);
+        if (is_device_ptr(n_neg)) MGB_CUDA(cudaMemcpy(n_neg, cnt_h.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice));
+        else std::memcpy(n_neg, cnt_h.data(), sizeof(int32_t) * E);
+        sgd_copy_back(*a, c, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}

@@ -1,0 +1,636 @@
+// Sampled SGD layout on the device: optimize_layout of src/layout.cpp:343-472 (epoch_worker :118-276,
+// apply_step :90-116, run_epochs :281-339).
+//
+// Two stream modes:
+//  * counter-based (stream_mode 0, default): every sampled edge of an epoch draws from its own xorshift64*
+//    stream, seeded with the reference's formula (src/layout.cpp:123) with tid = edge index, so draws need no
+//    coordination. With the edges sorted by head (the reference's schedule is the COO of a sorted CSR) one
+//    thread owns each head row and applies the head's steps one after another in registers, as the reference's
+//    loop does; tails and partners move through hogwild float atomics.
+//  * serial (stream_mode 1): the reference's single stream per epoch (n_threads = 1) is replayed exactly. The
+//    schedule (eons / eonns) is computed in parallel; one thread walks the sampled edges in order to find where
+//    each edge's draws start in the stream (its RNG state is recorded), then the head rows run in parallel from
+//    their recorded states in 8 sub-steps per epoch (sub-step p: the p-th sampled edge of every row). Within a
+//    sub-step every position is read as committed by the previous one and all displacements are summed in 2^-32
+//    fixed point (order-independent integer atomics), so the result does not depend on scheduling: the same
+//    inputs give the same bits on every run.
+//    Assumption stated for the replay: no negative sample lands at exactly the head's position (distance 0);
+//    the reference draws extra uniforms in that case (src/layout.cpp:181), which the replay does not.
+#include "sgd.cuh"
+#include <vector>
+#include <cmath>
+#include <algorithm>
+
+namespace mgb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr double kFix = 4294967296.0;   // 2^32
+
+int blocks_for(int64_t work, int per_block, int cap_per_sm = 16) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((work + per_block - 1) / per_block, (int64_t)cap_per_sm * kNumSMs));
+}
+
+// ---------------------------------------------------------------------------------------------- step sinks
+// apply_step (src/layout.cpp:90-116): optional lazy Adam, step = alpha * g, clip per coordinate at 4 alpha or
+// by norm, y += step. The sinks differ in how y += step lands.
+template <int D>
+__device__ __forceinline__ void make_step(const SgdDev& c, const float* g, float alpha, int64_t node, int dim,
+                                          float* step) {
+    if (c.optimizer == 1) {
+        const int32_t t = atomicAdd(&c.adam_t[node], 1) + 1;
+        const float c1 = 1.0f - powf(c.beta1, (float)t), c2 = 1.0f - powf(c.beta2, (float)t);
+        float* m = c.adam_m + node * dim;
+        float* v = c.adam_v + node * dim;
+        for (int d = 0; d < dim; ++d) {
+            const float md = c.beta1 * m[d] + (1.0f - c.beta1) * g[d];
+            const float vd = c.beta2 * v[d] + (1.0f - c.beta2) * g[d] * g[d];
+            m[d] = md; v[d] = vd;
+            step[d] = alpha * (md / c1) / (sqrtf(vd / c2) + 1e-7f);
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+            if (d < dim) step[d] = __fmul_rn(alpha, g[d]);
+    }
+    const float cap = 4.0f * alpha;
+    if (c.clip_mode == 1) {
+        float n2 = 0.0f;
+        for (int d = 0; d < dim; ++d) n2 = __fadd_rn(n2, __fmul_rn(step[d], step[d]));
+        if (n2 > cap * cap) {
+            const float f = cap / sqrtf(n2);
+            for (int d = 0; d < dim; ++d) step[d] *= f;
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+            if (d < dim) step[d] = step[d] > cap ? cap : (step[d] < -cap ? -cap : step[d]);
+    }
+}
+
+struct HogwildSink {
+    template <int D>
+    __device__ __forceinline__ void apply(const SgdDev& c, int64_t node, const float* g, float alpha, int dim) const {
+        float step[D];
+        make_step<D>(c, g, alpha, node, dim, step);
+        if (D == 2) {
+            atomicAdd(reinterpret_cast<float2*>(c.Y) + node, make_float2(step[0], step[1]));
+        } else {
+            for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[node * dim + d], step[d]);
+        }
+    }
+};
+
+struct FixedSink {
+    unsigned long long* delta;
+    template <int D>
+    __device__ __forceinline__ void apply(const SgdDev& c, int64_t node, const float* g, float alpha, int dim) const {
+        float step[D];
+        make_step<D>(c, g, alpha, node, dim, step);
+        for (int d = 0; d < dim; ++d)
+            atomicAdd(&delta[node * dim + d], (unsigned long long)llrint((double)step[d] * kFix));
+    }
+};
+
+struct NullSink {
+    template <int D>
+    __device__ __forceinline__ void apply(const SgdDev&, int64_t, const float*, float, int) const {}
+};
+
+// Optional record of the draws (schedule test hook)
+struct Rec {
+    int32_t* negs;       // at neg_off[i]
+    const int64_t* neg_off;
+    int64_t negs_cap;
+    int32_t* mid;        // per edge
+};
+
+// ---------------------------------------------------------------------------------------------- the edge
+// One sampled edge of epoch_worker (src/layout.cpp:136-274) for the hogwild semantics, with the draws taken
+// from `rng` in the reference's order. n_neg is the number of negatives of this sample (computed by the
+// caller from the schedule). Positions are read from c.Y.
+// Local apply_step of the head: the head's position lives in registers of the thread that owns its row, so its
+// steps follow one another as in the reference's sequential loop.
+template <int D>
+__device__ __forceinline__ void local_step(const SgdDev& c, float* yu, const float* g, float alpha, int64_t node,
+                                           int dim) {
+    float step[D];
+    make_step<D>(c, g, alpha, node, dim, step);
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+        if (d < dim) yu[d] += step[d];
+}
+
+// yu: the head's current position (updated in place when the head moves); Y: where the other rows are read
+template <int D, class Sink>
+__device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_neg, float alpha, float mid_w, Rng& rng,
+                                             const Sink& sink, const Rec* rec, float* yu, const float* Y) {
+    const int dim = D == 0 ? c.dim : D;
+    constexpr int DM = D == 0 ? kMaxDim : D;
+    const int32_t u = c.head[i], v = c.tail[i];
+    float diff[DM], gu[DM], gk[DM];
+    const bool move_u = u >= c.n_fixed, move_v = v >= c.n_fixed;
+    float d2 = 0.0f;
+    for (int d = 0; d < dim; ++d) {
+        diff[d] = yu[d] - Y[(int64_t)v * dim + d];
+        d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d]));
+        gu[d] = 0.0f;
+    }
+    const float b_u = c.node_b ? c.node_b[u] : c.b;
+    const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
+    const float pw_v = (c.b_is_one && !c.node_b) ? d2 : (d2 > 0.0f ? powf(d2, b_uv) : 0.0f);
+    int64_t rec_at = rec ? rec->neg_off[i] : 0;
+    if (c.loss == 0) {
+        if (d2 > 0.0f) {
+            float coeff;
+            const float s = -c.exaggeration;
+            if (c.kernel == 0) coeff = s * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
+            else if (c.kernel == 1) coeff = s * 2.0f * c.a;
+            else if (c.kernel == 2) { const float dd = sqrtf(d2); coeff = s * c.a * tanhf(c.a * dd) / dd; }
+            else coeff = s * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
+            for (int d = 0; d < dim; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
+            if (move_v) sink.template apply<DM>(c, v, gk, alpha, dim);
+        }
+        for (int p = 0; p < n_neg; ++p) {
+            const int32_t k = (int32_t)rng.below((uint32_t)c.n);
+            if (rec) { if (rec_at < rec->negs_cap) rec->negs[rec_at] = k; ++rec_at; }
+            if (k == u) continue;
+            float dd = 0.0f;
+            for (int d = 0; d < dim; ++d) {
+                diff[d] = yu[d] - Y[(int64_t)k * dim + d];
+                dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d]));
+            }
+            if (dd > 0.0f) {
+                float coeff;
+                if (c.kernel == 0) {
+                    if (c.node_b && c.rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f)); }
+                    else { const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b); coeff = c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f)); }
+                } else if (c.kernel == 1) {
+                    const float q = expf(-c.a * dd);
+                    coeff = c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
+                } else if (c.kernel == 2) {
+                    const float r = sqrtf(dd); const float q = 1.0f / coshf(c.a * r);
+                    coeff = c.repulsion_strength * c.a * q * tanhf(c.a * r) / (r * fmaxf(1.0f - q, 1e-3f));
+                } else {
+                    const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
+                    coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
+                }
+                for (int d = 0; d < dim; ++d) gu[d] += coeff * diff[d];
+            } else {
+                for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+            }
+        }
+    } else {
+        // InfoNCE (src/layout.cpp:185-223); the negatives are moved too
+        int32_t negs[64]; float qk[64];
+        const float q_v = 1.0f / (1.0f + c.a * pw_v);
+        float Z = q_v;
+        for (int p = 0; p < c.m_neg; ++p) {
+            int32_t k = (int32_t)rng.below((uint32_t)c.n);
+            if (k == u) k = (int32_t)((k + 1) % c.n);
+            negs[p] = k;
+            if (rec) { if (rec_at < rec->negs_cap) rec->negs[rec_at] = k; ++rec_at; }
+            float dd = 0.0f;
+            for (int d = 0; d < dim; ++d) { const float t = yu[d] - Y[(int64_t)k * dim + d]; dd = __fadd_rn(dd, __fmul_rn(t, t)); }
+            const float pw = c.b_is_one ? dd : (dd > 0.0f ? powf(dd, c.b) : 0.0f);
+            qk[p] = 1.0f / (1.0f + c.a * pw);
+            Z += qk[p];
+        }
+        const float w_v = q_v / Z;
+        if (d2 > 0.0f) {
+            const float coeff = -c.exaggeration * (1.0f - w_v) * c.two_ab * pw_v / (d2 * (c.a * pw_v + 1.0f));
+            for (int d = 0; d < dim; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
+            if (move_v) sink.template apply<DM>(c, v, gk, alpha, dim);
+        }
+        for (int p = 0; p < c.m_neg; ++p) {
+            const int32_t k = negs[p];
+            float dd = 0.0f;
+            for (int d = 0; d < dim; ++d) { diff[d] = yu[d] - Y[(int64_t)k * dim + d]; dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d])); }
+            if (dd <= 0.0f) {
+                for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                continue;
+            }
+            const float pw = c.b_is_one ? dd : powf(dd, c.b);
+            const float w_k = qk[p] / Z;
+            const float coeff = c.repulsion_strength * w_k * c.two_ab * pw / (dd * (c.a * pw + 1.0f));
+            for (int d = 0; d < dim; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
+            if (k >= c.n_fixed) sink.template apply<DM>(c, k, gk, alpha, dim);
+        }
+    }
+    // mid-range partner (src/layout.cpp:225-255)
+    if (mid_w > 0.0f && rng.uniform() < c.mid_rate) {
+        int32_t w = v;
+        if (c.jump_indptr) {
+            const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
+            for (int h = 0; h < L; ++h) {
+                const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
+                if (je > js && rng.uniform() < c.mid_jump) {
+                    w = c.jump_indices[js + (int32_t)rng.below((uint32_t)(je - js))];
+                } else {
+                    const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                    if (e0 <= s0) break;
+                    w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
+                }
+            }
+        } else if (c.mid_pairs) {
+            w = c.mid_pairs[(int64_t)u * c.n_mid + rng.below((uint32_t)c.n_mid)];
+        } else {
+            const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
+            for (int h = 0; h < L; ++h) {
+                const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                if (e0 <= s0) break;
+                w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
+            }
+        }
+        if (rec) rec->mid[i] = (w != u) ? w : -2;
+        if (w != u) {
+            for (int d = 0; d < dim; ++d) {
+                const float g = -mid_w * (yu[d] - Y[(int64_t)w * dim + d]);
+                gu[d] += g; gk[d] = -g;
+            }
+            if (w >= c.n_fixed) sink.template apply<DM>(c, w, gk, alpha, dim);
+        }
+    }
+    if (move_u) local_step<DM>(c, yu, gu, alpha, u, dim);
+}
+
+// Schedule of one sample (src/layout.cpp:135, 160-163, 184; InfoNCE :221-222): returns n_neg or -1 when the
+// edge is not sampled this epoch, and advances eons / eonns.
+__device__ __forceinline__ int schedule_edge(const SgdDev& c, int64_t i, float fepoch) {
+    const float eon = c.eons[i];
+    if (eon > fepoch) return -1;
+    const float eps = c.eps[i];
+    c.eons[i] = __fadd_rn(eon, eps);
+    if (c.loss == 0) {
+        const float epn = eps / c.negative_sample_rate;
+        const float eonn = c.eonns[i];
+        const int n_neg = (int)((fepoch - eonn) / epn);
+        c.eonns[i] = __fadd_rn(eonn, __fmul_rn((float)n_neg, epn));
+        return n_neg > 0 ? n_neg : 0;
+    }
+    c.eonns[i] = fepoch;
+    return c.m_neg;
+}
+
+// ---------------------------------------------------------------------------------------------- kernels
+template <int D>
+__device__ __forceinline__ void load_row(const float* Y, int64_t u, int dim, float* yu) {
+#pragma unroll
+    for (int d = 0; d < (D == 0 ? kMaxDim : D); ++d)
+        if (d < dim) yu[d] = Y[u * dim + d];
+}
+
+// Row kernel, hogwild: one thread owns head u and walks its edges in order (edges sorted by head, row pointers
+// eptr). The head's steps accumulate in registers one after another, as in the reference's loop; the tail,
+// mid-range partner (and InfoNCE negatives) move through float atomics. The head's total displacement lands with
+// one atomic at the end, on top of whatever the other rows added to it meanwhile.
+template <int D>
+__global__ void __launch_bounds__(kThreads) hogwild_rows_kernel(SgdDev c, const int64_t* __restrict__ eptr, int epoch,
+                                                                float alpha, float mid_w) {
+    const int dim = D == 0 ? c.dim : D;
+    constexpr int DM = D == 0 ? kMaxDim : D;
+    const float fepoch = (float)epoch;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < c.n; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e0 = eptr[u], e1 = eptr[u + 1];
+        if (e0 == e1) continue;
+        float yu[DM], y0[DM];
+        bool any = false;
+        for (int64_t i = e0; i < e1; ++i) {
+            const int n_neg = schedule_edge(c, i, fepoch);
+            if (n_neg < 0) continue;
+            if (!any) { load_row<D>(c.Y, u, dim, yu); for (int d = 0; d < dim; ++d) y0[d] = yu[d]; any = true; }
+            Rng rng(stream_seed(c.seed, epoch, (uint64_t)i));
+            process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y);
+        }
+        if (!any || u < c.n_fixed) continue;
+        if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
+        else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
+    }
+}
+
+// Edge kernel, hogwild (edges not sorted by head): one thread per edge; the head's step lands with an atomic.
+template <int D>
+__global__ void __launch_bounds__(kThreads) hogwild_edges_kernel(SgdDev c, int epoch, float alpha, float mid_w) {
+    const int dim = D == 0 ? c.dim : D;
+    constexpr int DM = D == 0 ? kMaxDim : D;
+    const float fepoch = (float)epoch;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges; i += (int64_t)gridDim.x * blockDim.x) {
+        const int n_neg = schedule_edge(c, i, fepoch);
+        if (n_neg < 0) continue;
+        const int64_t u = c.head[i];
+        float yu[DM], y0[DM];
+        load_row<D>(c.Y, u, dim, yu);
+        for (int d = 0; d < dim; ++d) y0[d] = yu[d];
+        Rng rng(stream_seed(c.seed, epoch, (uint64_t)i));
+        process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y);
+        if (u < c.n_fixed) continue;
+        if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
+        else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
+    }
+}
+
+// serial stream, phase 1: the schedule of the epoch (parallel); cnt[i] = n_neg or -1
+__global__ void serial_schedule_kernel(SgdDev c, int epoch, int32_t* __restrict__ cnt) {
+    const float fepoch = (float)epoch;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges; i += (int64_t)gridDim.x * blockDim.x)
+        cnt[i] = schedule_edge(c, i, fepoch);
+}
+
+// serial stream, phase 2: one thread walks the sampled edges in order through the epoch's single stream
+// (seed tid 0) and records the generator state at the start of each sampled edge. It consumes the draws of
+// each sample as the reference does: n_neg (or m_neg) below() calls, then with a mid weight one uniform() and,
+// on success, the partner draws (a pair index, or the steps of the walk).
+__global__ void serial_chain_kernel(SgdDev c, int epoch, float mid_w, const int32_t* __restrict__ cnt,
+                                    uint64_t* __restrict__ state) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    Rng rng(stream_seed(c.seed, epoch, 0));
+    for (int64_t i = 0; i < c.n_edges; ++i) {
+        const int k = cnt[i];
+        if (k < 0) continue;
+        state[i] = rng.s;
+        for (int p = 0; p < k; ++p) rng.next();
+        if (mid_w > 0.0f && rng.uniform() < c.mid_rate) {
+            int32_t w = c.tail[i];
+            if (c.jump_indptr) {
+                const int L = c.walk_lens ? c.walk_lens[c.tail[i]] : c.walk_len;
+                for (int h = 0; h < L; ++h) {
+                    const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
+                    if (je > js && rng.uniform() < c.mid_jump) {
+                        w = c.jump_indices[js + (int32_t)rng.below((uint32_t)(je - js))];
+                    } else {
+                        const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                        if (e0 <= s0) break;
+                        w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
+                    }
+                }
+            } else if (c.mid_pairs) {
+                rng.next();
+            } else {
+                const int L = c.walk_lens ? c.walk_lens[c.tail[i]] : c.walk_len;
+                for (int h = 0; h < L; ++h) {
+                    const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                    if (e0 <= s0) break;
+                    w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
+                }
+            }
+        }
+    }
+}
+
+// serial stream, phase 3 (rows), in kSerialPhases sub-steps: sub-step p processes the p-th sampled edge of every
+// head row (the last sub-step the rest of the row, in order) from its recorded state, reading every position as
+// committed after the previous sub-step; the displacements of the sub-step are summed in fixed point and
+// committed before the next one. Each sub-step's result is a function of its inputs only, and the reads are
+// never older than one sub-step (about one edge sample per head) instead of one epoch.
+constexpr int kSerialPhases = 8;
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) serial_rows_kernel(SgdDev c, const int64_t* __restrict__ eptr, int phase,
+                                                               float alpha, float mid_w,
+                                                               const int32_t* __restrict__ cnt,
+                                                               const uint64_t* __restrict__ state,
+                                                               unsigned long long* __restrict__ delta) {
+    const int dim = D == 0 ? c.dim : D;
+    constexpr int DM = D == 0 ? kMaxDim : D;
+    const FixedSink sink{delta};
+    const bool last = phase == kSerialPhases - 1;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < c.n; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e0 = eptr[u], e1 = eptr[u + 1];
+        float yu[DM], y0[DM];
+        bool any = false;
+        int seen = 0;
+        for (int64_t i = e0; i < e1; ++i) {
+            const int k = cnt[i];
+            if (k < 0) continue;
+            const int idx = seen++;
+            if (idx < phase) continue;
+            if (!any) { load_row<D>(c.Y, u, dim, yu); for (int d = 0; d < dim; ++d) y0[d] = yu[d]; any = true; }
+            Rng rng(0);
+            rng.s = state[i];
+            process_edge<D>(c, i, k, alpha, mid_w, rng, sink, nullptr, yu, c.Y);
+            if (!last) break;
+        }
+        if (!any || u < c.n_fixed) continue;
+        for (int d = 0; d < dim; ++d)
+            atomicAdd(&delta[u * dim + d], (unsigned long long)llrint((double)(yu[d] - y0[d]) * kFix));
+    }
+}
+
+// serial stream, phase 3 (edges not sorted by head): one thread per sampled edge against the snapshot
+template <int D>
+__global__ void __launch_bounds__(kThreads) serial_edges_kernel(SgdDev c, const float* __restrict__ Ysnap,
+                                                                float alpha, float mid_w,
+                                                                const int32_t* __restrict__ cnt,
+                                                                const uint64_t* __restrict__ state,
+                                                                unsigned long long* __restrict__ delta) {
+    const int dim = D == 0 ? c.dim : D;
+    constexpr int DM = D == 0 ? kMaxDim : D;
+    const FixedSink sink{delta};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges; i += (int64_t)gridDim.x * blockDim.x) {
+        const int k = cnt[i];
+        if (k < 0) continue;
+        const int64_t u = c.head[i];
+        float yu[DM], y0[DM];
+        load_row<D>(Ysnap, u, dim, yu);
+        for (int d = 0; d < dim; ++d) y0[d] = yu[d];
+        Rng rng(0);
+        rng.s = state[i];
+        process_edge<D>(c, i, k, alpha, mid_w, rng, sink, nullptr, yu, Ysnap);
+        if (u < c.n_fixed) continue;
+        for (int d = 0; d < dim; ++d)
+            atomicAdd(&delta[u * dim + d], (unsigned long long)llrint((double)(yu[d] - y0[d]) * kFix));
+    }
+}
+
+// serial stream, phase 4: y = snapshot + delta * 2^-32 (the snapshot is the layout itself), delta = 0
+__global__ void commit_kernel(float* __restrict__ Y, unsigned long long* __restrict__ delta, int64_t total) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        const long long q = (long long)delta[k];
+        if (q != 0) {
+            Y[k] = (float)((double)Y[k] + (double)q * (1.0 / kFix));
+            delta[k] = 0ull;
+        }
+    }
+}
+
+// row pointers of an edge list sorted by head: eptr[u] = first edge with head >= u
+__global__ void row_ptr_kernel(const int32_t* __restrict__ head, int64_t E, int64_t n, int64_t* __restrict__ eptr) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u <= n; u += (int64_t)gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = E;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (head[mid] < u) lo = mid + 1; else hi = mid;
+        }
+        eptr[u] = lo;
+    }
+}
+
+__global__ void unsorted_kernel(const int32_t* __restrict__ head, int64_t E, int* __restrict__ flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < E; i += (int64_t)gridDim.x * blockDim.x)
+        if (head[i] < head[i - 1]) { *flag = 1; return; }
+}
+
+// schedule hook: the draws of one epoch (no updates)
+template <int D>
+__global__ void record_kernel(SgdDev c, int epoch, float alpha, float mid_w, const int32_t* __restrict__ cnt,
+                              const uint64_t* __restrict__ state, int per_edge, Rec rec) {
+    const int dim = D == 0 ? c.dim : D;
+    constexpr int DM = D == 0 ? kMaxDim : D;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges; i += (int64_t)gridDim.x * blockDim.x) {
+        rec.mid[i] = -1;
+        const int k = cnt[i];
+        if (k < 0) continue;
+        Rng rng(0);
+        if (per_edge) rng = Rng(stream_seed(c.seed, epoch, (uint64_t)i));
+        else rng.s = state[i];
+        float yu[DM];
+        load_row<D>(c.Y, c.head[i], dim, yu);
+        process_edge<D>(c, i, k, alpha, mid_w, rng, NullSink(), &rec, yu, c.Y);
+    }
+}
+
+// exclusive prefix sum of max(cnt, 0) (single block; test hook sizes)
+__global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64_t* __restrict__ off, int64_t* total) {
+    __shared__ int64_t carry;
+    __shared__ int64_t wsum[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < n; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        int64_t v = (i < n && cnt[i] > 0) ? cnt[i] : 0;
+        int64_t x = v;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { const int64_t y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int64_t w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { const int64_t y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const int64_t incl = x + (warp > 0 ? wsum[warp - 1] : 0);
+        if (i < n) off[i] = carry + incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+template <int D>
+void hogwild_epoch(const SgdDev& c, const int64_t* eptr, int epoch, float alpha, float mid_w, cudaStream_t s) {
+    if (eptr) hogwild_rows_kernel<D><<<blocks_for(c.n, kThreads), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
+    else hogwild_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, alpha, mid_w);
+}
+template <int D>
+void serial_apply(const SgdDev& c, const int64_t* eptr, float alpha, float mid_w, const int32_t* cnt,
+                  const uint64_t* st, unsigned long long* delta, cudaStream_t s) {
+    const int64_t total = c.n * c.dim;
+    if (!eptr) {
+        serial_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, c.Y, alpha, mid_w, cnt, st, delta);
+        MGB_LAUNCH_CHECK();
+        commit_kernel<<<blocks_for(total, kThreads), kThreads, 0, s>>>(c.Y, delta, total);
+        return;
+    }
+    for (int p = 0; p < kSerialPhases; ++p) {
+        serial_rows_kernel<D><<<blocks_for(c.n, kThreads), kThreads, 0, s>>>(c, eptr, p, alpha, mid_w, cnt, st, delta);
+        MGB_LAUNCH_CHECK();
+        commit_kernel<<<blocks_for(total, kThreads), kThreads, 0, s>>>(c.Y, delta, total);
+        if (p + 1 < kSerialPhases) MGB_LAUNCH_CHECK();
+    }
+}
+template <int D>
+void record_launch(const SgdDev& c, int epoch, float alpha, float mid_w, const int32_t* cnt, const uint64_t* st,
+                   int per_edge, Rec rec, cudaStream_t s) {
+    record_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, alpha, mid_w, cnt, st, per_edge, rec);
+}
+
+#define MGB_DIM_DISPATCH(dim, F, ...)                \
+    switch (dim) {                                   \
+        case 2: F<2>(__VA_ARGS__); break;            \
+        case 3: F<3>(__VA_ARGS__); break;            \
+        default: F<0>(__VA_ARGS__); break;           \
+    }
+
+// row pointers when the edges are sorted by head (the reference's schedule is the COO of a sorted CSR), else
+// nullptr (edge-parallel kernels)
+const int64_t* row_pointers(const SgdDev& c, SgdWork& w, cudaStream_t s) {
+    if (c.n_edges == 0) return nullptr;
+    int* flag = static_cast<int*>(w.flag.ensure(sizeof(int)));
+    MGB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+    unsorted_kernel<<<blocks_for(c.n_edges, kThreads, 4), kThreads, 0, s>>>(c.head, c.n_edges, flag);
+    MGB_LAUNCH_CHECK();
+    int h = 0;
+    MGB_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MGB_CUDA(cudaStreamSynchronize(s));
+    if (h) return nullptr;
+    int64_t* eptr = static_cast<int64_t*>(w.eptr.ensure(sizeof(int64_t) * (c.n + 1)));
+    row_ptr_kernel<<<blocks_for(c.n + 1, kThreads, 4), kThreads, 0, s>>>(c.head, c.n_edges, c.n, eptr);
+    MGB_LAUNCH_CHECK();
+    return eptr;
+}
+
+}  // namespace
+
+void sgd_sched(const SgdDev& c, int epoch, int e0, int e1, float alpha0, float alpha1, float mid_w0, float mid_w1,
+               float& alpha, float& mid_w) {
+    // run_epochs' linear schedule inside a call (src/layout.cpp:284-289)
+    const int n_span = std::max(1, e1 - e0);
+    const float frac = (float)(epoch - e0) / (float)n_span;
+    alpha = alpha0 + (alpha1 - alpha0) * frac;
+    mid_w = c.use_mid ? mid_w0 + (mid_w1 - mid_w0) * frac : 0.0f;
+}
+
+void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha0, float alpha1, float mid_w0,
+             float mid_w1, cudaStream_t s) {
+    const int64_t* eptr = row_pointers(c, w, s);
+    if (stream_mode == 0) {
+        for (int e = e0; e < e1; ++e) {
+            float alpha, mid_w;
+            sgd_sched(c, e, e0, e1, alpha0, alpha1, mid_w0, mid_w1, alpha, mid_w);
+            MGB_DIM_DISPATCH(c.dim, hogwild_epoch, c, eptr, e, alpha, mid_w, s);
+            MGB_LAUNCH_CHECK();
+        }
+        return;
+    }
+    int32_t* cnt = static_cast<int32_t*>(w.cnt.ensure(sizeof(int32_t) * std::max<int64_t>(c.n_edges, 1)));
+    uint64_t* st = static_cast<uint64_t*>(w.state.ensure(sizeof(uint64_t) * std::max<int64_t>(c.n_edges, 1)));
+    const int64_t total = c.n * c.dim;
+    unsigned long long* delta = static_cast<unsigned long long*>(w.delta.ensure(sizeof(unsigned long long) * total));
+    MGB_CUDA(cudaMemsetAsync(delta, 0, sizeof(unsigned long long) * total, s));
+    for (int e = e0; e < e1; ++e) {
+        float alpha, mid_w;
+        sgd_sched(c, e, e0, e1, alpha0, alpha1, mid_w0, mid_w1, alpha, mid_w);
+        serial_schedule_kernel<<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, e, cnt);
+        MGB_LAUNCH_CHECK();
+        serial_chain_kernel<<<1, 32, 0, s>>>(c, e, mid_w, cnt, st);
+        MGB_LAUNCH_CHECK();
+        MGB_DIM_DISPATCH(c.dim, serial_apply, c, eptr, alpha, mid_w, cnt, st, delta, s);
+        MGB_LAUNCH_CHECK();
+    }
+}
+
+void sgd_record(SgdDev& c, SgdWork& w, int stream_mode, int epoch, float alpha, float mid_w, int32_t* n_neg_out,
+                int64_t* off_out, int32_t* negs, int64_t negs_cap, int32_t* mid, int64_t* n_negs_dev,
+                cudaStream_t s) {
+    int32_t* cnt = static_cast<int32_t*>(w.cnt.ensure(sizeof(int32_t) * std::max<int64_t>(c.n_edges, 1)));
+    uint64_t* st = static_cast<uint64_t*>(w.state.ensure(sizeof(uint64_t) * std::max<int64_t>(c.n_edges, 1)));
+    serial_schedule_kernel<<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, cnt);
+    MGB_LAUNCH_CHECK();
+    if (stream_mode == 1) {
+        serial_chain_kernel<<<1, 32, 0, s>>>(c, epoch, mid_w, cnt, st);
+        MGB_LAUNCH_CHECK();
+    }
+    MGB_CUDA(cudaMemcpyAsync(n_neg_out, cnt, sizeof(int32_t) * c.n_edges, cudaMemcpyDeviceToDevice, s));
+    offsets_kernel<<<1, 1024, 0, s>>>(cnt, c.n_edges, off_out, n_negs_dev);
+    MGB_LAUNCH_CHECK();
+    Rec rec{negs, off_out, negs_cap, mid};
+    MGB_DIM_DISPATCH(c.dim, record_launch, c, epoch, alpha, mid_w, cnt, st, stream_mode == 0 ? 1 : 0, rec, s);
+    MGB_LAUNCH_CHECK();
+}
+
+}  // namespace mgb

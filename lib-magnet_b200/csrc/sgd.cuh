@@ -1,0 +1,40 @@
+// Sampled SGD layout on the device (optimize_layout, src/layout.cpp:343-472).
+#pragma once
+#include "common.cuh"
+
+namespace mgb {
+
+// Everything an epoch kernel reads (the reference's Ctx, src/layout.cpp:69-88), as device pointers plus the
+// scalars derived once per call (src/layout.cpp:421-431).
+struct SgdDev {
+    float* Y; int64_t n; int dim;
+    const int32_t* head; const int32_t* tail; const float* eps; float* eons; float* eonns; int64_t n_edges;
+    const int32_t* indptr; const int32_t* indices; const int32_t* walk_lens;
+    const int32_t* mid_pairs; int n_mid;
+    const int32_t* jump_indptr; const int32_t* jump_indices; float mid_jump;
+    float a, b, two_ab, two_b, negative_sample_rate, exaggeration, repulsion_strength, mid_rate;
+    float rep_a, rep_b;
+    bool b_is_one, rep_b_is_one, rep_coupled, use_mid;
+    int m_neg, walk_len, loss, clip_mode, kernel, optimizer;
+    int64_t n_fixed;
+    const float* node_b;
+    float* adam_m; float* adam_v; int32_t* adam_t; float beta1, beta2;
+    uint64_t seed;
+};
+
+// device scratch of the serial stream mode
+struct SgdWork {
+    DevBuf cnt, state, delta, eptr, flag;
+};
+
+void sgd_sched(const SgdDev& c, int epoch, int e0, int e1, float alpha0, float alpha1, float mid_w0, float mid_w1,
+               float& alpha, float& mid_w);
+// epochs [e0, e1) (one optimize_layout call), asynchronous on s
+void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha0, float alpha1, float mid_w0,
+             float mid_w1, cudaStream_t s);
+// draws of one epoch without updates (device outputs); advances eons / eonns
+void sgd_record(SgdDev& c, SgdWork& w, int stream_mode, int epoch, float alpha, float mid_w, int32_t* n_neg_out,
+                int64_t* off_out, int32_t* negs, int64_t negs_cap, int32_t* mid, int64_t* n_negs_dev,
+                cudaStream_t s);
+
+}  // namespace mgb

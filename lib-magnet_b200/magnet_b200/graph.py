@@ -1,0 +1,152 @@
+"""Host-side inputs of the layout pass: the fuzzy neighbour graph, mid-near partners and the initial layout.
+
+These steps are upstream of the layout pass; the reference runs them on the host (NN-descent, smooth kNN,
+fuzzy union, mid-near pairs, spectral / PCA init) and so does this package. They are restated here, from the
+reference's behaviour, so that workloads can be built where the reference is not installed:
+
+* ``smooth_knn``: UMAP's per-row bandwidth search (src/graph.cpp:29-78, magnet/knn.py:165-198);
+* ``fuzzy_graph``: the fuzzy union A + A^T - A o A^T (magnet/knn.py:215-230);
+* ``exact_knn``: exact k nearest neighbours (self excluded, sorted) by blocked matmul on a CUDA device when
+  torch sees one, else numpy; it stands in for NN-descent (src/nndescent.cpp), whose output it bounds;
+* ``mid_near_pairs``: PaCMAP-style partners, the second closest of n_cand random rows (src/nndescent.cpp:731-759);
+* ``initial_layout``: the reference's rescale of an initial embedding (magnet/__init__.py:444-448).
+"""
+import numpy as np
+import scipy.sparse as sp
+
+
+def smooth_knn(dist, n_neighbors, bandwidth=1.0, n_iter=64):
+    """dist (n, k) sorted neighbour distances (self excluded) -> memberships (n, k) in (0, 1]; vectorised over rows,
+    float32 as the reference's kernel."""
+    dist = np.asarray(dist, dtype=np.float32)
+    n, k = dist.shape
+    target = np.float32(np.log2(np.float32(n_neighbors)) * np.float32(bandwidth))
+    nonzero = dist > 0
+    has = nonzero.any(1)
+    first = np.argmax(nonzero, axis=1)
+    rho = np.where(has, dist[np.arange(n), first], np.float32(0)).astype(np.float32)
+    dmr = dist - rho[:, None]
+    lo = np.zeros(n, np.float32)
+    hi = np.full(n, np.inf, np.float32)
+    mid = np.ones(n, np.float32)
+    sigma = np.ones(n, np.float32)
+    done = np.zeros(n, bool)
+    for _ in range(n_iter):
+        psum = np.where(dmr > 0, np.exp(-dmr / mid[:, None]), np.float32(1)).astype(np.float32).sum(1, dtype=np.float32)
+        newly = (~done) & (np.abs(psum - target) < 1e-5)
+        sigma[newly] = mid[newly]
+        done |= newly
+        if done.all():
+            break
+        gt = psum > target
+        hi = np.where(done, hi, np.where(gt, mid, hi))
+        lo = np.where(done, lo, np.where(gt, lo, mid))
+        mid = np.where(done, mid, np.where(gt, (lo + hi) * np.float32(0.5),
+                                           np.where(np.isinf(hi), mid * np.float32(2), (lo + hi) * np.float32(0.5))))
+        mid = mid.astype(np.float32)
+    sigma[~done] = mid[~done]
+    mean_row = dist.astype(np.float64).sum(1) / k
+    sigma = np.where(rho > 0, np.maximum(sigma, np.float32(1e-3) * mean_row.astype(np.float32)), sigma)
+    mean_all = np.float32(dist.astype(np.float64).sum() / (n * k))
+    sigma = np.where(rho > 0, sigma, np.maximum(sigma, np.float32(1e-3) * mean_all)).astype(np.float32)
+    return np.where(dmr > 0, np.exp(-dmr / sigma[:, None]), np.float32(1)).astype(np.float32)
+
+
+def fuzzy_graph(ind, dist, n_neighbors, n=None, set_op_mix_ratio=1.0):
+    """symmetric fuzzy neighbourhood graph (CSR float32, sorted indices, no diagonal)"""
+    n = ind.shape[0] if n is None else n
+    vals = smooth_knn(dist, n_neighbors)
+    rows = np.repeat(np.arange(n, dtype=np.int64), ind.shape[1])
+    A = sp.csr_matrix((vals.ravel(), (rows, np.asarray(ind).ravel())), shape=(n, n), dtype=np.float32)
+    A.eliminate_zeros()
+    T = A.T.tocsr()
+    prod = A.multiply(T)
+    P = set_op_mix_ratio * (A + T - prod) + (1.0 - set_op_mix_ratio) * prod
+    P = sp.csr_matrix(P, dtype=np.float32)
+    P.setdiag(0)
+    P.eliminate_zeros()
+    P.sort_indices()
+    return P
+
+
+def exact_knn(X, k, block=2048):
+    """(indices (n, k-1) int64, distances (n, k-1) float32) of the k-1 nearest other rows, sorted"""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n = X.shape[0]
+    kk = min(k, n)
+    try:
+        import torch
+        cuda = torch.cuda.is_available()
+    except ImportError:
+        cuda = False
+    if cuda:
+        import torch
+        prev = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = False
+        Xd = torch.from_numpy(X).cuda()
+        sq = (Xd * Xd).sum(1)
+        I = np.empty((n, kk), np.int64)
+        D = np.empty((n, kk), np.float32)
+        for s in range(0, n, block):
+            q = Xd[s:s + block]
+            d2 = sq[s:s + block, None] - 2.0 * (q @ Xd.T) + sq[None, :]
+            d2[torch.arange(q.shape[0], device=q.device), torch.arange(s, s + q.shape[0], device=q.device)] = float("inf")
+            v, i = torch.topk(d2, kk - 1, dim=1, largest=False, sorted=True)
+            I[s:s + block, :kk - 1] = i.cpu().numpy()
+            D[s:s + block, :kk - 1] = torch.sqrt(torch.clamp(v, min=0.0)).cpu().numpy()
+        torch.backends.cuda.matmul.allow_tf32 = prev
+        return I[:, :kk - 1], D[:, :kk - 1]
+    sq = (X.astype(np.float64) ** 2).sum(1)
+    I = np.empty((n, kk - 1), np.int64)
+    D = np.empty((n, kk - 1), np.float32)
+    for s in range(0, n, block):
+        d2 = sq[s:s + block, None] - 2.0 * (X[s:s + block].astype(np.float64) @ X.T.astype(np.float64)) + sq[None, :]
+        d2[np.arange(d2.shape[0]), np.arange(s, s + d2.shape[0])] = np.inf
+        part = np.argpartition(d2, kk - 1, axis=1)[:, :kk - 1]
+        pd = np.take_along_axis(d2, part, 1)
+        o = np.argsort(pd, 1)
+        I[s:s + block] = np.take_along_axis(part, o, 1)
+        D[s:s + block] = np.sqrt(np.maximum(np.take_along_axis(pd, o, 1), 0)).astype(np.float32)
+    return I, D
+
+
+def mid_near_pairs(X, n_pairs=5, n_cand=6, seed=0, block=65536):
+    """(n, n_pairs) int32: for every row and pair, the second closest of n_cand random other rows"""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n = X.shape[0]
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, n_pairs), np.int32)
+    for s in range(0, n, block):
+        e = min(n, s + block)
+        rows = np.arange(s, e)
+        cand = rng.integers(0, n - 1, (e - s, n_pairs, n_cand))
+        cand = cand + (cand >= rows[:, None, None])          # never the row itself
+        d = ((X[cand] - X[rows][:, None, None, :]) ** 2).sum(-1)
+        second = np.argsort(d, axis=-1)[..., 1]
+        out[s:e] = np.take_along_axis(cand, second[..., None], -1)[..., 0]
+    return out
+
+
+def pca2(X, seed=0):
+    """2-D PCA projection (randomised range finder; the t-SNE mode's init)"""
+    X = np.asarray(X, dtype=np.float32)
+    Xc = X - X.mean(0)
+    rng = np.random.default_rng(seed)
+    G = rng.normal(size=(X.shape[1], 8)).astype(np.float32)
+    Q, _ = np.linalg.qr(Xc @ G)
+    for _ in range(2):
+        Q, _ = np.linalg.qr(Xc @ (Xc.T @ Q))
+    B = Q.T @ Xc
+    _, _, Vt = np.linalg.svd(B, full_matrices=False)
+    return (Xc @ Vt[:2].T).astype(np.float32)
+
+
+def initial_layout(Y, seed=0):
+    """centred, scaled to max-abs 10, plus N(0, 1e-4) jitter (magnet/__init__.py:444-448)"""
+    Y = np.array(Y, dtype=np.float32)
+    Y -= Y.mean(0)
+    scale = np.abs(Y).max()
+    if scale > 0:
+        Y *= 10.0 / scale
+    Y += np.random.default_rng(seed).normal(0, 1e-4, Y.shape).astype(np.float32)
+    return np.ascontiguousarray(Y, dtype=np.float32)

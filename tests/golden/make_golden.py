@@ -1,0 +1,142 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself (kerighan/lib-magnet 3.0.2).
+
+Runs only where the reference checkout is available (default /root/reference, override with
+MAGNET_REFERENCE_DIR) and its native module has been compiled by oracle/build_ref.sh. Every output is produced
+by the reference's own code: its compiled `_magnet` (optimize_layout at n_threads=1, FFTConv2D, tsne_attraction,
+tsne_step, bbox_2d) and its Python drivers (magnet/tsne.py FFTRepulsion2D / optimize_tsne, magnet/knn.py
+fuzzy_graph, magnet/__init__.py edge schedule). Inputs are seeded synthetic data.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+import scipy.sparse as sp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("MAGNET_REFERENCE_DIR", "/root/reference")
+sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))   # the compiled reference module, importable as _magnet
+sys.path.insert(0, REF)
+
+import _magnet  # noqa: E402  (the reference's native module)
+from magnet import MAGNET  # noqa: E402
+from magnet.knn import fuzzy_graph  # noqa: E402
+from magnet.tsne import FFTRepulsion2D, optimize_tsne  # noqa: E402
+
+
+def knn_graph(X, k):
+    """exact kNN (self excluded) -> the reference's fuzzy graph"""
+    D = ((X[:, None, :] - X[None, :, :]) ** 2).sum(-1)
+    np.fill_diagonal(D, np.inf)
+    ind = np.argsort(D, 1)[:, :k - 1]
+    dist = np.sqrt(np.take_along_axis(D, ind, 1)).astype(np.float32)
+    return fuzzy_graph(ind, dist, k)
+
+
+def blobs(n, d, centers, seed, scale=5.0):
+    rng = np.random.default_rng(seed)
+    y = rng.integers(0, centers, n)
+    C = rng.normal(0, scale, (centers, d))
+    return (C[y] + rng.normal(0, 1, (n, d))).astype(np.float32), y
+
+
+def sgd_fixture():
+    X, y = blobs(600, 10, 5, seed=11)
+    P = knn_graph(X, 15)
+    n_epochs = 40
+    est = MAGNET(n_epochs=n_epochs, random_state=0)
+    head, tail, eps = est._edge_schedule(P, n_epochs)
+    rng = np.random.default_rng(5)
+    Y0 = rng.uniform(-10, 10, (600, 2)).astype(np.float32)
+    mid_pairs = rng.integers(0, 600, (600, 5)).astype(np.int32)
+    z = np.zeros(0, np.int32)
+    out = dict(X=X, labels=y, head=head, tail=tail, eps=eps, Y0=Y0, mid_pairs=mid_pairs,
+               indptr=P.indptr.astype(np.int32), indices=P.indices.astype(np.int32), data=P.data.astype(np.float32))
+    cases = {
+        "default": dict(b=0.8, mid=1, walk=0),
+        "b1": dict(b=1.0, mid=0, walk=0),
+        "walk": dict(b=0.8, mid=0, walk=1),
+    }
+    for name, cfg in cases.items():
+        Y = Y0.copy(); eons = eps.copy(); eonns = (eps / 5).astype(np.float32)
+        mp = mid_pairs if cfg["mid"] else np.zeros((0, 1), np.int32)
+        mw = 0.1 if (cfg["mid"] or cfg["walk"]) else 0.0
+        ip = out["indptr"] if cfg["walk"] else z
+        ix = out["indices"] if cfg["walk"] else z
+        _magnet.optimize_layout(Y, head, tail, eps, eons, eonns, ip, ix, 0, n_epochs, 1.0, 0.0, mw, 0.0,
+                                1.7, cfg["b"], 1.7382, 1.0, 5.0, 0, 1.0, 2.0, 4, 0.25, 0, 0, 0,
+                                np.zeros((0, 2), np.float32), np.zeros((0, 2), np.float32), z, 0.9, 0.999, z, mp, z, z,
+                                0.0, 0, np.zeros(0, np.float32), 12345, 1, 0)
+        out[f"Y_{name}"] = Y
+        out[f"eons_{name}"] = eons
+        out[f"eonns_{name}"] = eonns
+    np.savez_compressed(os.path.join(HERE, "sgd_small.npz"), **out)
+
+
+def fft_fixture():
+    out = {}
+    # the reference's own test vector (tests/test_magnet.py:221-231): n = 1500, N(0, 8^2), seed 0, n_interp = 5
+    rng = np.random.default_rng(0)
+    Y = np.ascontiguousarray(rng.normal(0, 8, (1500, 2)).astype(np.float32))
+    for ni in (5, 3):
+        rep = FFTRepulsion2D(n_interp=ni, n_threads=1)
+        xmin, ymin, width, nb = rep._grid(Y)
+        M, K1h, K2h = rep._kernels(nb, width)
+        sumQ, F = rep(Y)
+        out[f"grid_{ni}"] = np.array([xmin, ymin, width, nb], np.float64)
+        out[f"M_{ni}"] = np.array(M)
+        # the spectra themselves are not stored (megabytes); their checksums pin oracle.kernel_spectra
+        out[f"K1h_sum_{ni}"] = np.array([np.float64(K1h.real).sum(), np.abs(np.float64(K1h.real)).max()])
+        out[f"K2h_sum_{ni}"] = np.array([np.float64(K2h.real).sum(), np.abs(np.float64(K2h.real)).max()])
+        out[f"sumQ_{ni}"] = np.array(sumQ, np.float64)
+        out[f"F_{ni}"] = F.astype(np.float32)
+    D2 = ((Y[:, None, :].astype(np.float64) - Y[None, :, :]) ** 2).sum(-1)
+    Q = 1.0 / (1.0 + D2)
+    np.fill_diagonal(Q, 0)
+    out["sumQ_exact"] = np.array(Q.sum())
+    out["F_exact"] = ((Q ** 2)[:, :, None] * (Y[:, None, :].astype(np.float64) - Y[None, :, :])).sum(1)
+    out["Y"] = Y
+    # a t-SNE-like clustered layout (the grid's dense / sparse mix), n = 4000, n_interp = 3
+    Yc, _ = blobs(4000, 2, 8, seed=3, scale=12.0)
+    rep = FFTRepulsion2D(n_interp=3, n_threads=1)
+    sumQ, F = rep(Yc)
+    out["Yc"] = Yc
+    out["sumQ_c"] = np.array(sumQ, np.float64)
+    out["F_c"] = F.astype(np.float32)
+    out["grid_c"] = np.array(rep._grid(Yc), np.float64)
+    np.savez_compressed(os.path.join(HERE, "fft_small.npz"), **out)
+
+
+def tsne_fixture():
+    X, y = blobs(1200, 10, 6, seed=21)
+    P = knn_graph(X, 15)
+    rng = np.random.default_rng(2)
+    Y0 = (rng.normal(0, 1, (1200, 2)) * 1e-4).astype(np.float32)
+    Pn = sp.csr_matrix(P, dtype=np.float32)
+    Pn = Pn / Pn.sum()
+    ip, ix, dd = Pn.indptr.astype(np.int32), Pn.indices.astype(np.int32), Pn.data.astype(np.float32)
+    Yl = (rng.normal(0, 6, (1200, 2))).astype(np.float32)
+    attr = np.asarray(_magnet.tsne_attraction(ip, ix, dd, Yl, 1.0, 1))
+    attr07 = np.asarray(_magnet.tsne_attraction(ip, ix, dd, Yl, 0.7, 1))
+    bbox = np.array(_magnet.bbox_2d(Yl, 1), np.float32)
+    U = rng.normal(0, 0.1, (1200, 2)).astype(np.float32)
+    G = rng.uniform(0.5, 2.0, (1200, 2)).astype(np.float32)
+    Fr = rng.normal(0, 1, (1200, 2)).astype(np.float32)
+    Ys, Us, Gs = Yl.copy(), U.copy(), G.copy()
+    _magnet.tsne_step(Ys, Us, Gs, attr, Fr, 12.0, 1e-3, 250.0, 0.5, 1)
+    Yt = optimize_tsne(P, Y0.copy(), n_iter=60, early_iter=20, n_threads=1)
+    np.savez_compressed(os.path.join(HERE, "tsne_small.npz"), X=X, labels=y,
+                        indptr=P.indptr.astype(np.int32), indices=P.indices.astype(np.int32),
+                        data=P.data.astype(np.float32), Y0=Y0, Yl=Yl, attr=attr, attr07=attr07, bbox=bbox,
+                        U=U, G=G, Fr=Fr, Ys=Ys, Us=Us, Gs=Gs, Y_tsne60=Yt)
+
+
+if __name__ == "__main__":
+    sgd_fixture()
+    fft_fixture()
+    tsne_fixture()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))

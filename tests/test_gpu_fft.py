@@ -1,0 +1,83 @@
+"""FFT-interpolated repulsion on the device against the reference (FFTConv2D.compute of the compiled reference,
+golden vectors it produced) and against the FP64 all-pairs oracle. Tolerance: sumQ and F within 1e-4 relative
+(F as a norm over the points) of the reference; the interpolation error against the exact sums within the
+reference's own bounds (tests/test_magnet.py:230-231)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def fftconv(mg, Y, grid, ni):
+    xmin, ymin, width, nb = grid
+    M, K1, K2 = O.kernel_spectra(int(nb), float(width), ni)
+    conv = mg.FFTConv2D(M, ni)
+    conv.set_kernels(K1, K2)
+    return conv.compute(np.ascontiguousarray(Y, np.float32), float(xmin), float(ymin), float(width), int(nb))
+
+
+@pytest.mark.parametrize("ni", [5, 3])
+def test_reference_test_vector(mg, golden, ni):
+    g = golden("fft_small.npz")
+    sq, F = fftconv(mg, g["Y"], g[f"grid_{ni}"], ni)
+    assert abs(sq - g[f"sumQ_{ni}"]) / g[f"sumQ_{ni}"] < TOL
+    assert np.linalg.norm(F - g[f"F_{ni}"]) / np.linalg.norm(g[f"F_{ni}"]) < TOL
+    assert abs(sq - g["sumQ_exact"]) / g["sumQ_exact"] < 1e-3
+    assert np.linalg.norm(F - g["F_exact"]) / np.linalg.norm(g["F_exact"]) < 2e-2
+
+
+def test_clustered_layout(mg, golden):
+    g = golden("fft_small.npz")
+    sq, F = fftconv(mg, g["Yc"], g["grid_c"], 3)
+    assert abs(sq - g["sumQ_c"]) / g["sumQ_c"] < TOL
+    assert np.linalg.norm(F - g["F_c"]) / np.linalg.norm(g["F_c"]) < TOL
+
+
+@pytest.mark.parametrize("n,scale", [(20000, 25.0), (70000, 31.0)])
+def test_against_compiled_reference(mg, ref, n, scale):
+    if ref is None:
+        pytest.skip("reference module not built")
+    rng = np.random.default_rng(n)
+    Y = (rng.standard_t(3, (n, 2)) * scale / 3).astype(np.float32)
+    grid = O.grid(Y)
+    M, K1, K2 = O.kernel_spectra(grid[3], grid[2], 3)
+    conv_r = ref.FFTConv2D(M, 3)
+    conv_r.set_kernels(K1, K2)
+    sq_r, F_r = conv_r.compute(Y, grid[0], grid[1], grid[2], grid[3], -1)
+    sq, F = fftconv(mg, Y, grid, 3)
+    F_r = np.asarray(F_r)
+    assert abs(sq - sq_r) / sq_r < TOL
+    assert np.linalg.norm(F - F_r) / np.linalg.norm(F_r) < TOL
+
+
+def test_precision_against_fp64_all_pairs(mg):
+    """FP32 spread / FFT / gather against the direct FP64 sums at n = 10,000 (the precision study's oracle)"""
+    rng = np.random.default_rng(7)
+    Y = (rng.normal(0, 20, (10000, 2))).astype(np.float32)
+    grid = O.grid(Y)
+    sq, F = fftconv(mg, Y, grid, 3)
+    sq_e, F_e = O.exact_repulsion(Y)
+    assert abs(sq - sq_e) / sq_e < 1e-3
+    assert np.linalg.norm(F - F_e) / np.linalg.norm(F_e) < 2e-2
+
+
+def test_device_tensors_in_place(mg, golden):
+    import torch
+    g = golden("fft_small.npz")
+    xmin, ymin, width, nb = g["grid_3"]
+    M, K1, K2 = O.kernel_spectra(int(nb), float(width), 3)
+    conv = mg.FFTConv2D(M, 3)
+    conv.set_kernels(K1, K2)
+    Yd = torch.from_numpy(g["Y"]).cuda()
+    sq, Fd = conv.compute(Yd, float(xmin), float(ymin), float(width), int(nb))
+    assert Fd.is_cuda
+    assert np.linalg.norm(Fd.cpu().numpy() - g["F_3"]) / np.linalg.norm(g["F_3"]) < TOL
+
+
+def test_grid_too_large_raises(mg):
+    conv = mg.FFTConv2D(120, 3)
+    with pytest.raises(RuntimeError, match="grid larger than the buffer"):
+        conv.compute(np.zeros((10, 2), np.float32), 0.0, 0.0, 0.7, 60)
