@@ -50,6 +50,11 @@ void RepBuffers::alloc(int Nmax_, int Mmax_, int ni_) {
     }
     fft_len_table.ensure(table.size() * sizeof(int));
     MGB_CUDA(cudaMemcpy(fft_len_table.p, table.data(), table.size() * sizeof(int), cudaMemcpyHostToDevice));
+    use2 = fft2_fits(Mmax);
+    if (use2) {
+        fft2_build_plans(plans, Mmax);
+        ensure_fft2_attrs();
+    }
 }
 
 namespace {
@@ -471,6 +476,10 @@ void ensure_fft_attrs() {
 }
 
 void rep_convolve(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEvent_t* ev) {
+    if (b.use2) {
+        rep_convolve2(g, b, n, s, ev);
+        return;
+    }
     const size_t smem = fft_smem(b.Mmax);
     const int pairs = (b.Nmax + 1) / 2;
     row_fwd_kernel<<<fft_blocks(pairs), kFftThreads, smem, s>>>(g, b.W.as<float4>(), b.Nmax, b.WhT.as<float2>(),
@@ -504,6 +513,10 @@ void rep_prepare_device_spectra(RepBuffers& b) {
 void rep_update_spectra(GridDesc* g, RepBuffers& b, float dof, cudaStream_t s) {
     const int Pa = b.Mmax / 2 + 1;
     require(b.Rt.p != nullptr, "rep_prepare_device_spectra must run first");
+    if (b.use2) {
+        rep_update_spectra2(g, b, dof, s);
+        return;
+    }
     const size_t smem = fft_smem(b.Mmax);
     spec_rows_kernel<<<fft_blocks(Pa), kFftThreads, smem, s>>>(g, b.Rt.as<float2>(), Pa, b.Mhmax, b.tw.as<float2>(),
                                                                 b.ni, (double)dof);

@@ -35,8 +35,9 @@ struct GridDesc {
 
 struct RepBuffers {
     int Nmax = 0, Mmax = 0, Mhmax = 0, Npmax = 0, ni = 3;
-    DevBuf W, WhT, PhT, phi, Kt, Rt, tw, zpart, fft_len_table, bbox_part, mean_part;
+    DevBuf W, WhT, PhT, phi, Kt, Rt, tw, zpart, fft_len_table, bbox_part, mean_part, plans;
     int max_bbox_blocks = 0;
+    bool use2 = false;        // the register-tiled FFT engine (fftrep2.cu) holds this Mmax
     void alloc(int Nmax_, int Mmax_, int ni_);
 };
 
@@ -54,6 +55,13 @@ void rep_gather_forces(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, f
 void rep_set_spectra_from_host_layout(RepBuffers& b, const float* K1h_dev, const float* K2h_dev, int M,
                                       cudaStream_t s);
 void rep_twiddles(GridDesc* g, RepBuffers& b, cudaStream_t s, bool force);   // recompute tw if g->tw_dirty
+
+// register-tiled engine (fftrep2.cu)
+bool fft2_fits(int Mmax);
+void fft2_build_plans(DevBuf& table, int Mmax);
+void ensure_fft2_attrs();
+void rep_convolve2(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEvent_t* ev);
+void rep_update_spectra2(GridDesc* g, RepBuffers& b, float dof, cudaStream_t s);
 
 // the whole t-SNE iteration pieces (tsne.cu)
 struct TsneDev;

@@ -110,6 +110,14 @@ struct Rec {
 // One sampled edge of epoch_worker (src/layout.cpp:136-274) for the hogwild semantics, with the draws taken
 // from `rng` in the reference's order. n_neg is the number of negatives of this sample (computed by the
 // caller from the schedule). Positions are read from c.Y.
+// Side stream of the distance-0 jitter in the per-edge stream mode: negative p of a sample draws its jitter
+// uniforms here, so that the main stream holds exactly the negatives, the mid-range draw and the partner draws
+// and any draw of a sample can be taken directly by position (the reference draws the jitter from the main
+// stream, src/layout.cpp:181; the serial stream mode keeps that order).
+__host__ __device__ __forceinline__ Rng jitter_rng(uint64_t sseed, int p) {
+    return Rng(sseed ^ 0xA24BAED4963EE407ULL ^ ((uint64_t)(p + 1) * 0x9FB21C651E98DF25ULL));
+}
+
 // Local apply_step of the head: the head's position lives in registers of the thread that owns its row, so its
 // steps follow one another as in the reference's sequential loop.
 template <int D>
@@ -123,9 +131,11 @@ __device__ __forceinline__ void local_step(const SgdDev& c, float* yu, const flo
 }
 
 // yu: the head's current position (updated in place when the head moves); Y: where the other rows are read
+// split_jitter: the per-edge stream mode (jitter from jitter_rng(sseed, p)); otherwise the reference's order
 template <int D, class Sink>
 __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_neg, float alpha, float mid_w, Rng& rng,
-                                             const Sink& sink, const Rec* rec, float* yu, const float* Y) {
+                                             const Sink& sink, const Rec* rec, float* yu, const float* Y,
+                                             bool split_jitter = false, uint64_t sseed = 0) {
     const int dim = D == 0 ? c.dim : D;
     constexpr int DM = D == 0 ? kMaxDim : D;
     const int32_t u = c.head[i], v = c.tail[i];
@@ -177,6 +187,9 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
                     coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
                 }
                 for (int d = 0; d < dim; ++d) gu[d] += coeff * diff[d];
+            } else if (split_jitter) {
+                Rng jr = jitter_rng(sseed, p);
+                for (int d = 0; d < dim; ++d) gu[d] += (jr.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
             } else {
                 for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
             }
@@ -208,7 +221,12 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
             float dd = 0.0f;
             for (int d = 0; d < dim; ++d) { diff[d] = yu[d] - Y[(int64_t)k * dim + d]; dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d])); }
             if (dd <= 0.0f) {
-                for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                if (split_jitter) {
+                    Rng jr = jitter_rng(sseed, p);
+                    for (int d = 0; d < dim; ++d) gu[d] += (jr.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                } else {
+                    for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                }
                 continue;
             }
             const float pw = c.b_is_one ? dd : powf(dd, c.b);
@@ -300,12 +318,187 @@ __global__ void __launch_bounds__(kThreads) hogwild_rows_kernel(SgdDev c, const 
             const int n_neg = schedule_edge(c, i, fepoch);
             if (n_neg < 0) continue;
             if (!any) { load_row<D>(c.Y, u, dim, yu); for (int d = 0; d < dim; ++d) y0[d] = yu[d]; any = true; }
-            Rng rng(stream_seed(c.seed, epoch, (uint64_t)i));
-            process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y);
+            const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
+            Rng rng(ss);
+            process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y, true, ss);
         }
         if (!any || u < c.n_fixed) continue;
         if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
         else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
+    }
+}
+
+
+// Group kernel, hogwild, loss 0, dim 2 or 3: kGroup lanes own one head row. They read the row's schedule in
+// coalesced chunks of kGroup edges and ballot the sampled ones; each sample is then processed by the whole group:
+// negative p on lane p % (kGroup - 2) (lane p draws the p-th value of the edge's stream directly), the mid-range
+// partner on lane kGroup - 2, the attraction on lane kGroup - 1; the head's gradient is the group sum, and the
+// head's step is applied before the next sample, as in the reference's loop. Tails and partners move through
+// float2 atomics; the head's total displacement lands with one atomic at the end of the row.
+constexpr int kGroup = 8;
+
+template <int D>
+__device__ __forceinline__ float group_sum(float v, unsigned gmask) {
+#pragma unroll
+    for (int o = kGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o, kGroup);
+    return v;
+}
+
+template <int D>
+__device__ __forceinline__ void group_sample(const SgdDev& c, int64_t i, int32_t u, int n_neg, float alpha, float mid_w,
+                                             int epoch, int gl, unsigned gmask, float* yu) {
+    const int32_t v = c.tail[i];
+    const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
+    float gu[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) gu[d] = 0.0f;
+    constexpr int kNegLanes = kGroup - 2;
+    if (gl == kGroup - 1) {
+        // attraction (src/layout.cpp:149-159)
+        float diff[D], d2 = 0.0f;
+#pragma unroll
+        for (int d = 0; d < D; ++d) { diff[d] = yu[d] - c.Y[(int64_t)v * D + d]; d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d])); }
+        if (d2 > 0.0f) {
+            const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
+            const float pw_v = (c.b_is_one && !c.node_b) ? d2 : powf(d2, b_uv);
+            const float s = -c.exaggeration;
+            float coeff;
+            if (c.kernel == 0) coeff = s * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
+            else if (c.kernel == 1) coeff = s * 2.0f * c.a;
+            else if (c.kernel == 2) { const float dd = sqrtf(d2); coeff = s * c.a * tanhf(c.a * dd) / dd; }
+            else coeff = s * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
+            float gk[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
+            if (v >= c.n_fixed) HogwildSink().template apply<D>(c, v, gk, alpha, D);
+        }
+    } else if (gl == kGroup - 2) {
+        // mid-range partner (src/layout.cpp:225-255): draws n_neg and on of the stream
+        if (mid_w > 0.0f) {
+            Rng rng(ss);
+            for (int p = 0; p < n_neg; ++p) rng.next();
+            if (rng.uniform() < c.mid_rate) {
+                int32_t w = v;
+                if (c.jump_indptr) {
+                    const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
+                    for (int h = 0; h < L; ++h) {
+                        const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
+                        if (je > js && rng.uniform() < c.mid_jump) {
+                            w = c.jump_indices[js + (int32_t)rng.below((uint32_t)(je - js))];
+                        } else {
+                            const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                            if (e0 <= s0) break;
+                            w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
+                        }
+                    }
+                } else if (c.mid_pairs) {
+                    w = c.mid_pairs[(int64_t)u * c.n_mid + rng.below((uint32_t)c.n_mid)];
+                } else {
+                    const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
+                    for (int h = 0; h < L; ++h) {
+                        const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                        if (e0 <= s0) break;
+                        w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
+                    }
+                }
+                if (w != u) {
+                    float gk[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        const float g = -mid_w * (yu[d] - c.Y[(int64_t)w * D + d]);
+                        gu[d] += g; gk[d] = -g;
+                    }
+                    if (w >= c.n_fixed) HogwildSink().template apply<D>(c, w, gk, alpha, D);
+                }
+            }
+        }
+    }
+    // negatives (src/layout.cpp:164-183), negative p on lane p % kNegLanes
+    if (gl < kNegLanes && gl < n_neg) {
+        Rng rng(ss);
+        for (int p = 0; p < gl; ++p) rng.next();
+        const float b_u = c.node_b ? c.node_b[u] : c.b;
+        for (int p = gl; p < n_neg; p += kNegLanes) {
+            const int32_t k = (int32_t)rng.below((uint32_t)c.n);
+            for (int q = 1; q < kNegLanes; ++q) rng.next();
+            if (k == u) continue;
+            float diff[D], dd = 0.0f;
+#pragma unroll
+            for (int d = 0; d < D; ++d) { diff[d] = yu[d] - c.Y[(int64_t)k * D + d]; dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d])); }
+            if (dd > 0.0f) {
+                float coeff;
+                if (c.kernel == 0) {
+                    if (c.node_b && c.rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f)); }
+                    else { const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b); coeff = c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f)); }
+                } else if (c.kernel == 1) {
+                    const float q = expf(-c.a * dd);
+                    coeff = c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
+                } else if (c.kernel == 2) {
+                    const float r = sqrtf(dd); const float q = 1.0f / coshf(c.a * r);
+                    coeff = c.repulsion_strength * c.a * q * tanhf(c.a * r) / (r * fmaxf(1.0f - q, 1e-3f));
+                } else {
+                    const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
+                    coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
+                }
+#pragma unroll
+                for (int d = 0; d < D; ++d) gu[d] += coeff * diff[d];
+            } else {
+                Rng jr = jitter_rng(ss, p);
+#pragma unroll
+                for (int d = 0; d < D; ++d) gu[d] += (jr.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) gu[d] = group_sum<D>(gu[d], gmask);
+    if (u >= c.n_fixed) {
+        float step[D];
+        if (c.optimizer == 1) {
+            // lazy Adam of the head: one lane updates the state, the step is broadcast
+            if (gl == 0) make_step<D>(c, gu, alpha, u, D, step);
+#pragma unroll
+            for (int d = 0; d < D; ++d) step[d] = __shfl_sync(gmask, step[d], 0, kGroup);
+        } else {
+            make_step<D>(c, gu, alpha, u, D, step);
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) yu[d] += step[d];
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) hogwild_groups_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+                                                                  int epoch, float alpha, float mid_w) {
+    const int lane = threadIdx.x & 31;
+    const int gl = lane & (kGroup - 1);
+    const int gbase = lane & ~(kGroup - 1);
+    const unsigned gmask = ((1u << kGroup) - 1u) << gbase;
+    const float fepoch = (float)epoch;
+    const int64_t groups = (int64_t)gridDim.x * (blockDim.x / kGroup);
+    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x / kGroup) + threadIdx.x / kGroup; u < c.n; u += groups) {
+        const int64_t e0 = eptr[u], e1 = eptr[u + 1];
+        float yu[D], y0[D];
+        bool have = false;
+        for (int64_t base = e0; base < e1; base += kGroup) {
+            const int64_t i = base + gl;
+            const int nn = i < e1 ? schedule_edge(c, i, fepoch) : -1;
+            unsigned sm = (__ballot_sync(gmask, nn >= 0) >> gbase) & ((1u << kGroup) - 1u);
+            while (sm) {
+                const int src = __ffs(sm) - 1;
+                sm &= sm - 1;
+                const int n_neg = __shfl_sync(gmask, nn, src, kGroup);
+                if (!have) {
+#pragma unroll
+                    for (int d = 0; d < D; ++d) { yu[d] = c.Y[u * D + d]; y0[d] = yu[d]; }
+                    have = true;
+                }
+                group_sample<D>(c, base + src, (int32_t)u, n_neg, alpha, mid_w, epoch, gl, gmask, yu);
+            }
+        }
+        if (have && gl == 0 && u >= c.n_fixed) {
+            if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
+            else for (int d = 0; d < D; ++d) atomicAdd(&c.Y[u * D + d], yu[d] - y0[d]);
+        }
     }
 }
 
@@ -322,8 +515,9 @@ __global__ void __launch_bounds__(kThreads) hogwild_edges_kernel(SgdDev c, int e
         float yu[DM], y0[DM];
         load_row<D>(c.Y, u, dim, yu);
         for (int d = 0; d < dim; ++d) y0[d] = yu[d];
-        Rng rng(stream_seed(c.seed, epoch, (uint64_t)i));
-        process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y);
+        const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
+        Rng rng(ss);
+        process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y, true, ss);
         if (u < c.n_fixed) continue;
         if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
         else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
@@ -482,11 +676,12 @@ __global__ void record_kernel(SgdDev c, int epoch, float alpha, float mid_w, con
         const int k = cnt[i];
         if (k < 0) continue;
         Rng rng(0);
-        if (per_edge) rng = Rng(stream_seed(c.seed, epoch, (uint64_t)i));
+        const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
+        if (per_edge) rng = Rng(ss);
         else rng.s = state[i];
         float yu[DM];
         load_row<D>(c.Y, c.head[i], dim, yu);
-        process_edge<D>(c, i, k, alpha, mid_w, rng, NullSink(), &rec, yu, c.Y);
+        process_edge<D>(c, i, k, alpha, mid_w, rng, NullSink(), &rec, yu, c.Y, per_edge != 0, ss);
     }
 }
 
@@ -523,7 +718,9 @@ __global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64
 
 template <int D>
 void hogwild_epoch(const SgdDev& c, const int64_t* eptr, int epoch, float alpha, float mid_w, cudaStream_t s) {
-    if (eptr) hogwild_rows_kernel<D><<<blocks_for(c.n, kThreads), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
+    if (eptr && c.loss == 0 && (D == 2 || D == 3))
+        hogwild_groups_kernel<D == 0 ? 2 : D><<<blocks_for(c.n, kThreads / kGroup), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
+    else if (eptr) hogwild_rows_kernel<D><<<blocks_for(c.n, kThreads), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
     else hogwild_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, alpha, mid_w);
 }
 template <int D>

@@ -12,9 +12,9 @@
  *   orc_sgd_serial      src/layout.cpp:90-116 (apply_step), :118-276 (epoch_worker, hogwild path),
  *                       :281-297 (run_epochs, single-thread path), :343-472 (optimize_layout argument rules)
  *   orc_sgd_schedule    the draws epoch_worker makes (src/layout.cpp:123,135,160-166,184,226-249), recorded
- *                       instead of applied; stream_mode 0 = one stream per epoch (tid 0, the n_threads=1
- *                       reference), stream_mode 1 = one stream per edge (the GPU fast mode's counter-based
- *                       streams: the reference's seeding formula with tid = edge index)
+ *                       instead of applied; one stream per epoch (tid 0, the n_threads=1 reference), or one
+ *                       stream per edge (the device's fast mode: the reference's seeding formula with tid = edge
+ *                       index, and the distance-0 jitter drawn from a side stream per negative)
  *   orc_spread / orc_gather  src/fftconv.cpp:24-40 (lagrange_w), :83-123 (spread), :200-229 (gather)
  *   orc_tsne_attraction src/fftrep.cpp:129-177
  *   orc_tsne_step       src/fftrep.cpp:225-266 (one thread: nt = 1 partial sums, i.e. blocks of 1024 rows)
@@ -53,6 +53,12 @@ static inline float orc_rng_uniform(orc_rng* r) {
 /* epoch stream seed of src/layout.cpp:123 */
 static inline uint64_t orc_stream_seed(uint64_t seed, int epoch, uint64_t tid) {
     return seed * 0x9E3779B1ULL + (uint64_t)epoch * 0x85EBCA6BULL + tid * 0xC2B2AE35ULL;
+}
+
+/* per-edge stream mode: the distance-0 jitter of negative p comes from a side stream (the device's
+ * jitter_rng), so that the main stream holds only the negatives, the mid-range draw and the partner draws */
+static void orc_jitter_seed(orc_rng* r, uint64_t sseed, int p) {
+    orc_rng_seed(r, sseed ^ 0xA24BAED4963EE407ULL ^ ((uint64_t)(p + 1) * 0x9FB21C651E98DF25ULL));
 }
 
 /* exported for the RNG known-answer tests */
@@ -149,7 +155,8 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
     for (int64_t i = 0; i < c->n_edges; ++i) {
         if (rec) { rec->sampled[i] = 0; rec->n_neg[i] = 0; rec->mid[i] = -1; rec->neg_off[i] = rec->n_negs; }
         if (c->eons[i] > fepoch) continue;
-        if (per_edge_stream) orc_rng_seed(&rng, orc_stream_seed(c->seed, epoch, (uint64_t)i));
+        const uint64_t sseed = orc_stream_seed(c->seed, epoch, (uint64_t)i);
+        if (per_edge_stream) orc_rng_seed(&rng, sseed);
         if (rec) rec->sampled[i] = 1;
         const int32_t u = c->head[i], v = c->tail[i];
         float* yu = Y + (int64_t)u * dim;
@@ -200,6 +207,9 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
                         coeff = c->repulsion_strength * 2.0f * c->a * (1.0f - th * th) / th;
                     }
                     for (int q = 0; q < dim; ++q) gu[q] += coeff * diff[q];
+                } else if (per_edge_stream) {
+                    orc_rng jr; orc_jitter_seed(&jr, sseed, p);
+                    for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&jr) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
                 } else {
                     for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&rng) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
                 }
@@ -235,7 +245,12 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
                 float dd = 0.0f;
                 for (int q = 0; q < dim; ++q) { diff[q] = yu[q] - yk[q]; dd += diff[q] * diff[q]; }
                 if (dd <= 0.0f) {
-                    for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&rng) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                    if (per_edge_stream) {
+                        orc_rng jr; orc_jitter_seed(&jr, sseed, p);
+                        for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&jr) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                    } else {
+                        for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&rng) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                    }
                     continue;
                 }
                 const float pw = dv->b_is_one ? dd : powf(dd, c->b);
