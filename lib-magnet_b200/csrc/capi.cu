@@ -89,10 +89,14 @@ void validate_csr_host(const int32_t* ip, const int32_t* ix, int64_t nnz, int64_
         for (int64_t j = 0; j < nnz; ++j) require(ix[j] >= 0 && ix[j] < n_cols, "column index out of range");
 }
 
-__global__ void csr_sum_kernel(const float* __restrict__ P, int64_t nnz, double* __restrict__ out) {
+// sum of P in FP64: per-block partials, the last block adds them in block order (deterministic)
+__global__ void csr_sum_kernel(const float* __restrict__ P, int64_t nnz, double* __restrict__ part,
+                               unsigned* __restrict__ counter, double* __restrict__ out) {
     __shared__ double red[32];
+    __shared__ int is_last;
     double s = 0.0;
-    for (int64_t e = threadIdx.x; e < nnz; e += blockDim.x) s += (double)P[e];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+        s += (double)P[e];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -100,8 +104,17 @@ __global__ void csr_sum_kernel(const float* __restrict__ P, int64_t nnz, double*
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        *out = t;
+        part[blockIdx.x] = t;
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
+    __syncthreads();
+    if (!is_last || threadIdx.x != 0) return;
+    __threadfence();
+    double t = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) t += __ldcg(&part[b]);
+    *out = t;
+    *counter = 0u;
 }
 __global__ void csr_scale_kernel(const float* __restrict__ P, int64_t nnz, const double* __restrict__ sum,
                                  float* __restrict__ out) {
@@ -316,8 +329,13 @@ void tsne_prepare(TsneDev& d, const int32_t* indptr, const int32_t* indices, con
     d.init(ip, ix, Pd, n, nnz, false, sc, p.dof, p.threads_per_row, s);
     // P / P.sum() (magnet/tsne.py:149-150)
     if (nnz > 0) {
-        double* sum = static_cast<double*>(stage().scratch.ensure(sizeof(double)));
-        csr_sum_kernel<<<1, 1024, 0, s>>>(d.P.as<float>(), nnz, sum);
+        const int blocks = 2 * kNumSMs;
+        char* base = static_cast<char*>(stage().scratch.ensure(64 + sizeof(double) * (blocks + 1)));
+        unsigned* counter = reinterpret_cast<unsigned*>(base);
+        double* sum = reinterpret_cast<double*>(base + 8);
+        double* part = reinterpret_cast<double*>(base + 16);
+        MGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
+        csr_sum_kernel<<<blocks, 1024, 0, s>>>(d.P.as<float>(), nnz, part, counter, sum);
         MGB_LAUNCH_CHECK();
         csr_scale_kernel<<<256, 256, 0, s>>>(d.P.as<float>(), nnz, sum, d.P.as<float>());
         MGB_LAUNCH_CHECK();

@@ -28,6 +28,7 @@ inline void require(bool ok, const std::string& msg) {
     do {                                                                                                  \
         cudaError_t e_ = (call);                                                                          \
         if (e_ != cudaSuccess) {                                                                          \
+            cudaGetLastError(); /* a non-sticky error must not surface again at the next check */        \
             throw ::mgb::Error(e_ == cudaErrorMemoryAllocation ? MG_ERR_OUT_OF_MEMORY : MG_ERR_DEVICE,    \
                                std::string(#call) + ": " + cudaGetErrorString(e_));                      \
         }                                                                                                 \

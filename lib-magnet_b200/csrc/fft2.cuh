@@ -1,7 +1,8 @@
 // Register-tiled FFT engine of the repulsion pass: Stockham stages of large radices.
 //
-// A transform of length L = R1 R2 [R3 [R4]] runs as at most four Stockham stages. Each stage is a radix-R DFT
-// (R <= 32, a product of the base radices 2/3/4/5/8) held in the registers of one thread: R loads, inter-stage
+// A transform of length L = R1 R2 ... (at most five factors) runs as that many Stockham stages. Each stage is a
+// radix-R DFT (R <= 16: 2, 3, 4, 5, 6, 8, 9, 10, 12, 15, 16, products of the base radices 2/3/4/5/8) held in the
+// registers of one thread: R loads, inter-stage
 // twiddles, the DFT, R stores. Against the one-base-radix-per-stage engine this halves the number of passes
 // over shared memory; the first stage may read its input directly from global memory and the last may write
 // its output directly to global memory, which removes the staging passes too.
@@ -21,8 +22,8 @@
 namespace mgb {
 namespace fft2 {
 
-constexpr int kMaxStages = 4;
-constexpr int kMaxRadix = 32;
+constexpr int kMaxStages = 5;
+constexpr int kMaxRadix = 16;
 constexpr int kMaxLen = 13500;
 
 __host__ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
@@ -31,8 +32,7 @@ __host__ __device__ __forceinline__ int padded_len(int L) { return pad(L - 1) + 
 // the radices a stage may use
 __host__ __device__ inline bool is_radix(int r) {
     switch (r) {
-        case 2: case 3: case 4: case 5: case 6: case 8: case 9: case 10: case 12: case 15: case 16: case 18:
-        case 20: case 24: case 25: case 27: case 30: case 32: return true;
+        case 2: case 3: case 4: case 5: case 6: case 8: case 9: case 10: case 12: case 15: case 16: return true;
         default: return false;
     }
 }
@@ -44,40 +44,32 @@ struct Plan {
 };
 
 // Fewest stages; among equal counts, the most balanced radices (smallest largest radix). Host side; the device
-// loop reads plans from a table built here.
+// reads plans from a table built here.
+inline bool plan_search(int L, int depth, int* cur, int* best, int& best_n, int& best_max, int mx) {
+    static const int rad[] = {16, 15, 12, 10, 9, 8, 6, 5, 4, 3, 2};
+    if (L == 1) {
+        if (depth < best_n || (depth == best_n && mx < best_max)) {
+            best_n = depth; best_max = mx;
+            for (int s = 0; s < depth; ++s) best[s] = cur[s];
+        }
+        return true;
+    }
+    if (depth >= kMaxStages || depth + 1 > best_n) return false;
+    bool any = false;
+    for (int r : rad) {
+        if (L % r) continue;
+        cur[depth] = r;
+        any |= plan_search(L / r, depth + 1, cur, best, best_n, best_max, mx > r ? mx : r);
+    }
+    return any;
+}
+
 inline bool make_plan(int L, Plan& p) {
     p.L = L; p.n = 0;
     if (L < 2 || L > kMaxLen || !fft::is_5smooth(L)) return false;
-    static const int rad[] = {32, 30, 27, 25, 24, 20, 18, 16, 15, 12, 10, 9, 8, 6, 5, 4, 3, 2};
-    int best_n = 99, best_max = 99;
-    int best[kMaxStages] = {0, 0, 0, 0};
-    for (int a : rad) {
-        if (L % a) continue;
-        const int L1 = L / a;
-        if (L1 == 1) { if (1 < best_n || (1 == best_n && a < best_max)) { best_n = 1; best_max = a; best[0] = a; } continue; }
-        for (int b : rad) {
-            if (L1 % b) continue;
-            const int L2 = L1 / b;
-            if (L2 == 1) {
-                const int mx = a > b ? a : b;
-                if (2 < best_n || (2 == best_n && mx < best_max)) { best_n = 2; best_max = mx; best[0] = a; best[1] = b; }
-                continue;
-            }
-            for (int c : rad) {
-                if (L2 % c) continue;
-                const int L3 = L2 / c;
-                int mx = a > b ? a : b; mx = mx > c ? mx : c;
-                if (L3 == 1) {
-                    if (3 < best_n || (3 == best_n && mx < best_max)) { best_n = 3; best_max = mx; best[0] = a; best[1] = b; best[2] = c; }
-                    continue;
-                }
-                if (is_radix(L3)) {
-                    const int m4 = mx > L3 ? mx : L3;
-                    if (4 < best_n || (4 == best_n && m4 < best_max)) { best_n = 4; best_max = m4; best[0] = a; best[1] = b; best[2] = c; best[3] = L3; }
-                }
-            }
-        }
-    }
+    int cur[kMaxStages], best[kMaxStages];
+    int best_n = kMaxStages + 1, best_max = 1 << 30;
+    plan_search(L, 0, cur, best, best_n, best_max, 0);
     if (best_n > kMaxStages) return false;
     p.n = best_n;
     for (int s = 0; s < best_n; ++s) p.R[s] = best[s];
@@ -167,14 +159,7 @@ __device__ __forceinline__ void stage_dispatch(int R, const Load& ld, const Stor
         case 10: stage<10>(ld, st, L, Ns, tw, t0, nt); break;
         case 12: stage<12>(ld, st, L, Ns, tw, t0, nt); break;
         case 15: stage<15>(ld, st, L, Ns, tw, t0, nt); break;
-        case 16: stage<16>(ld, st, L, Ns, tw, t0, nt); break;
-        case 18: stage<18>(ld, st, L, Ns, tw, t0, nt); break;
-        case 20: stage<20>(ld, st, L, Ns, tw, t0, nt); break;
-        case 24: stage<24>(ld, st, L, Ns, tw, t0, nt); break;
-        case 25: stage<25>(ld, st, L, Ns, tw, t0, nt); break;
-        case 27: stage<27>(ld, st, L, Ns, tw, t0, nt); break;
-        case 30: stage<30>(ld, st, L, Ns, tw, t0, nt); break;
-        default: stage<32>(ld, st, L, Ns, tw, t0, nt); break;
+        default: stage<16>(ld, st, L, Ns, tw, t0, nt); break;
     }
 }
 

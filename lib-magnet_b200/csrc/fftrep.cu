@@ -417,7 +417,13 @@ int fft_blocks(int work) { return std::max(1, std::min(work, 2 * kNumSMs)); }
 size_t fft_smem(int M) { return (size_t)2 * M * sizeof(float2); }
 
 void set_smem_attr(const void* fn, size_t bytes) {
-    MGB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cudaFuncAttributes a;
+    MGB_CUDA(cudaFuncGetAttributes(&a, fn));
+    int dev = 0, optin = 0;
+    MGB_CUDA(cudaGetDevice(&dev));
+    MGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t mx = std::min(bytes, (size_t)optin - a.sharedSizeBytes);
+    MGB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
 }
 
 template <int NI>

@@ -90,7 +90,7 @@ struct RealStore {
 };
 
 // -------------------------------------------------------------------------------------------- kernels
-__global__ void __launch_bounds__(kT) row_fwd2_kernel(const GridDesc* __restrict__ gd, float4* __restrict__ W,
+__global__ void __launch_bounds__(kT, 2) row_fwd2_kernel(const GridDesc* __restrict__ gd, float4* __restrict__ W,
                                                       int pitchW, float2* __restrict__ WhT, int Np, int Mhmax,
                                                       const float2* __restrict__ tw,
                                                       const fft2::Plan* __restrict__ plans) {
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kT) row_fwd2_kernel(const GridDesc* __restrict
     }
 }
 
-__global__ void __launch_bounds__(kT) col2_kernel(GridDesc* __restrict__ gd, const float2* __restrict__ WhT,
+__global__ void __launch_bounds__(kT, 2) col2_kernel(GridDesc* __restrict__ gd, const float2* __restrict__ WhT,
                                                   float2* __restrict__ PhT, int Np, int Mhmax,
                                                   const float* __restrict__ Kt, int Mmax,
                                                   const float2* __restrict__ tw, double* __restrict__ zpart,
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kT) col2_kernel(GridDesc* __restrict__ gd, con
     }
 }
 
-__global__ void __launch_bounds__(kT) row_inv2_kernel(const GridDesc* __restrict__ gd,
+__global__ void __launch_bounds__(kT, 2) row_inv2_kernel(const GridDesc* __restrict__ gd,
                                                       const float2* __restrict__ PhT, int Np, int Mhmax,
                                                       float* __restrict__ phi, int pitchP,
                                                       const float2* __restrict__ tw,
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kT) row_inv2_kernel(const GridDesc* __restrict
     }
 }
 
-__global__ void __launch_bounds__(kT) spec_rows2_kernel(const GridDesc* __restrict__ gd, float2* __restrict__ Rt,
+__global__ void __launch_bounds__(kT, 2) spec_rows2_kernel(const GridDesc* __restrict__ gd, float2* __restrict__ Rt,
                                                         int Pa, int Mhmax, const float2* __restrict__ tw, int ni,
                                                         double dof, const fft2::Plan* __restrict__ plans) {
     if (!gd->spec_dirty) return;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kT) spec_rows2_kernel(const GridDesc* __restri
     }
 }
 
-__global__ void __launch_bounds__(kT) spec_cols2_kernel(const GridDesc* __restrict__ gd,
+__global__ void __launch_bounds__(kT, 2) spec_cols2_kernel(const GridDesc* __restrict__ gd,
                                                         const float2* __restrict__ Rt, int Pa, int Mhmax,
                                                         float* __restrict__ Kt, int Mmax,
                                                         const float2* __restrict__ tw,
@@ -279,22 +279,30 @@ int blocks2(int work) { return std::max(1, std::min(work, 2 * kNumSMs)); }
 
 }  // namespace
 
+// dynamic shared memory limit of a kernel: the device's opt-in maximum per block minus the kernel's static share
+static void raise_smem(const void* fn, int optin) {
+    cudaFuncAttributes a;
+    MGB_CUDA(cudaFuncGetAttributes(&a, fn));
+    MGB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes));
+}
+
 void ensure_fft2_attrs() {
     static int done_dev = -1;
     int dev = 0;
     MGB_CUDA(cudaGetDevice(&dev));
     if (done_dev == dev) return;
-    const int mx = 227 * 1024;
-    MGB_CUDA(cudaFuncSetAttribute((const void*)row_fwd2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    MGB_CUDA(cudaFuncSetAttribute((const void*)col2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    MGB_CUDA(cudaFuncSetAttribute((const void*)row_inv2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    MGB_CUDA(cudaFuncSetAttribute((const void*)spec_rows2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    MGB_CUDA(cudaFuncSetAttribute((const void*)spec_cols2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    int optin = 0;
+    MGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    raise_smem((const void*)row_fwd2_kernel, optin);
+    raise_smem((const void*)col2_kernel, optin);
+    raise_smem((const void*)row_inv2_kernel, optin);
+    raise_smem((const void*)spec_rows2_kernel, optin);
+    raise_smem((const void*)spec_cols2_kernel, optin);
     done_dev = dev;
 }
 
-// the register-tiled engine holds 3 padded sequences of length Mmax per block
-bool fft2_fits(int Mmax) { return (size_t)3 * fft2::padded_len(Mmax) * sizeof(float2) <= (size_t)227 * 1024; }
+// the register-tiled engine holds 3 padded sequences of length Mmax per block (1 KB left for static shared data)
+bool fft2_fits(int Mmax) { return (size_t)3 * fft2::padded_len(Mmax) * sizeof(float2) <= (size_t)226 * 1024; }
 
 void fft2_build_plans(DevBuf& table, int Mmax) {
     std::vector<fft2::Plan> plans((size_t)Mmax + 1);

@@ -2,11 +2,14 @@
 // apply_step :90-116, run_epochs :281-339).
 //
 // Two stream modes:
-//  * counter-based (stream_mode 0, default): every sampled edge of an epoch draws from its own xorshift64*
-//    stream, seeded with the reference's formula (src/layout.cpp:123) with tid = edge index, so draws need no
-//    coordination. With the edges sorted by head (the reference's schedule is the COO of a sorted CSR) one
-//    thread owns each head row and applies the head's steps one after another in registers, as the reference's
-//    loop does; tails and partners move through hogwild float atomics.
+//  * counter-based (stream_mode 0, default): every draw of a sample is addressed by (seed, epoch, edge, index).
+//    Draw j of edge i in epoch e is the first xorshift64* output of the generator seeded as the reference seeds
+//    its streams (src/layout.cpp:123, splitmix64 then xorshift64*) from stream_seed(seed, e, i) ^ (j * golden
+//    ratio). Negative p is draw p; the mid-range draws are draws 1024, 1025, ...; the distance-0 jitter of
+//    negative p in dimension d is draw 2048 + 64 p + d. Any lane can take any draw directly, so the draws of a
+//    sample need no coordination. With the edges sorted by head (the reference's schedule is the COO of a
+//    sorted CSR) a group of 8 lanes owns a head row and applies the head's steps one after another, as the
+//    reference's loop does; the tails and partners move through hogwild float2 atomics.
 //  * serial (stream_mode 1): the reference's single stream per epoch (n_threads = 1) is replayed exactly. The
 //    schedule (eons / eonns) is computed in parallel; one thread walks the sampled edges in order to find where
 //    each edge's draws start in the stream (its RNG state is recorded), then the head rows run in parallel from
@@ -27,14 +30,41 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr double kFix = 4294967296.0;   // 2^32
+constexpr int kMidDraw = 1024;          // first draw index of the mid-range draws (counter mode)
+constexpr int kJitterDraw = 2048;       // first draw index of the distance-0 jitter (counter mode)
 
 int blocks_for(int64_t work, int per_block, int cap_per_sm = 16) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((work + per_block - 1) / per_block, (int64_t)cap_per_sm * kNumSMs));
 }
 
-// ---------------------------------------------------------------------------------------------- step sinks
-// apply_step (src/layout.cpp:90-116): optional lazy Adam, step = alpha * g, clip per coordinate at 4 alpha or
-// by norm, y += step. The sinks differ in how y += step lands.
+// ---------------------------------------------------------------------------------------------- draws
+__device__ __forceinline__ uint32_t below_of(uint64_t x, uint32_t n) { return (uint32_t)(((x >> 32) * (uint64_t)n) >> 32); }
+__device__ __forceinline__ float uniform_of(uint64_t x) { return (float)(x >> 40) * (1.0f / 16777216.0f); }
+__device__ __forceinline__ uint64_t counter_draw(uint64_t ss, int j) {
+    Rng r(ss ^ ((uint64_t)j * 0x9E3779B97F4A7C15ULL));
+    return r.next();
+}
+
+// the reference's order: one stream, consumed in sequence
+struct SerialDraws {
+    Rng r;
+    __device__ __forceinline__ uint64_t neg() { return r.next(); }
+    __device__ __forceinline__ uint64_t mid() { return r.next(); }
+    __device__ __forceinline__ uint64_t jitter(int, int) { return r.next(); }
+};
+// the counter-based draws of the fast mode
+struct CounterDraws {
+    uint64_t ss;
+    int p = 0, t = 0;
+    __device__ __forceinline__ explicit CounterDraws(uint64_t s) : ss(s) {}
+    __device__ __forceinline__ uint64_t neg() { return counter_draw(ss, p++); }
+    __device__ __forceinline__ uint64_t mid() { return counter_draw(ss, kMidDraw + t++); }
+    __device__ __forceinline__ uint64_t jitter(int pi, int d) { return counter_draw(ss, kJitterDraw + 64 * pi + d); }
+};
+
+// ---------------------------------------------------------------------------------------------- steps
+// apply_step (src/layout.cpp:90-116): optional lazy Adam, step = alpha * g, clip per coordinate at 4 alpha or by
+// norm. The sinks differ in how y += step lands.
 template <int D>
 __device__ __forceinline__ void make_step(const SgdDev& c, const float* g, float alpha, int64_t node, int dim,
                                           float* step) {
@@ -74,11 +104,8 @@ struct HogwildSink {
     __device__ __forceinline__ void apply(const SgdDev& c, int64_t node, const float* g, float alpha, int dim) const {
         float step[D];
         make_step<D>(c, g, alpha, node, dim, step);
-        if (D == 2) {
-            atomicAdd(reinterpret_cast<float2*>(c.Y) + node, make_float2(step[0], step[1]));
-        } else {
-            for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[node * dim + d], step[d]);
-        }
+        if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + node, make_float2(step[0], step[1]));
+        else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[node * dim + d], step[d]);
     }
 };
 
@@ -98,28 +125,15 @@ struct NullSink {
     __device__ __forceinline__ void apply(const SgdDev&, int64_t, const float*, float, int) const {}
 };
 
-// Optional record of the draws (schedule test hook)
+// record of the draws (schedule test hook)
 struct Rec {
-    int32_t* negs;       // at neg_off[i]
+    int32_t* negs;          // at neg_off[i]
     const int64_t* neg_off;
     int64_t negs_cap;
-    int32_t* mid;        // per edge
+    int32_t* mid;           // per edge: -1 no mid-range draw succeeded, -2 the partner was the head, else the partner
 };
 
-// ---------------------------------------------------------------------------------------------- the edge
-// One sampled edge of epoch_worker (src/layout.cpp:136-274) for the hogwild semantics, with the draws taken
-// from `rng` in the reference's order. n_neg is the number of negatives of this sample (computed by the
-// caller from the schedule). Positions are read from c.Y.
-// Side stream of the distance-0 jitter in the per-edge stream mode: negative p of a sample draws its jitter
-// uniforms here, so that the main stream holds exactly the negatives, the mid-range draw and the partner draws
-// and any draw of a sample can be taken directly by position (the reference draws the jitter from the main
-// stream, src/layout.cpp:181; the serial stream mode keeps that order).
-__host__ __device__ __forceinline__ Rng jitter_rng(uint64_t sseed, int p) {
-    return Rng(sseed ^ 0xA24BAED4963EE407ULL ^ ((uint64_t)(p + 1) * 0x9FB21C651E98DF25ULL));
-}
-
-// Local apply_step of the head: the head's position lives in registers of the thread that owns its row, so its
-// steps follow one another as in the reference's sequential loop.
+// the head's own step, applied to its registers (the thread or group that owns the row holds its position)
 template <int D>
 __device__ __forceinline__ void local_step(const SgdDev& c, float* yu, const float* g, float alpha, int64_t node,
                                            int dim) {
@@ -130,12 +144,73 @@ __device__ __forceinline__ void local_step(const SgdDev& c, float* yu, const flo
         if (d < dim) yu[d] += step[d];
 }
 
-// yu: the head's current position (updated in place when the head moves); Y: where the other rows are read
-// split_jitter: the per-edge stream mode (jitter from jitter_rng(sseed, p)); otherwise the reference's order
-template <int D, class Sink>
-__device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_neg, float alpha, float mid_w, Rng& rng,
-                                             const Sink& sink, const Rec* rec, float* yu, const float* Y,
-                                             bool split_jitter = false, uint64_t sseed = 0) {
+// the mid-range partner of src/layout.cpp:226-249, after the mid-range uniform succeeded
+template <class Draws>
+__device__ __forceinline__ int32_t mid_partner(const SgdDev& c, int32_t u, int32_t v, Draws& dr) {
+    int32_t w = v;
+    if (c.jump_indptr) {
+        const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
+        for (int h = 0; h < L; ++h) {
+            const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
+            if (je > js && uniform_of(dr.mid()) < c.mid_jump) {
+                w = c.jump_indices[js + (int32_t)below_of(dr.mid(), (uint32_t)(je - js))];
+            } else {
+                const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+                if (e0 <= s0) break;
+                w = c.indices[s0 + (int32_t)below_of(dr.mid(), (uint32_t)(e0 - s0))];
+            }
+        }
+    } else if (c.mid_pairs) {
+        w = c.mid_pairs[(int64_t)u * c.n_mid + below_of(dr.mid(), (uint32_t)c.n_mid)];
+    } else {
+        const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
+        for (int h = 0; h < L; ++h) {
+            const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
+            if (e0 <= s0) break;
+            w = c.indices[s0 + (int32_t)below_of(dr.mid(), (uint32_t)(e0 - s0))];
+        }
+    }
+    return w;
+}
+
+// repulsion coefficient of a negative at squared distance dd > 0 (src/layout.cpp:166-179)
+__device__ __forceinline__ float repulsion_coeff(const SgdDev& c, float dd, int32_t u) {
+    if (c.kernel == 0) {
+        if (c.node_b && c.rep_coupled) {
+            const float b_u = c.node_b[u];
+            const float pw = powf(dd, b_u);
+            return 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f));
+        }
+        const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b);
+        return c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f));
+    }
+    if (c.kernel == 1) {
+        const float q = expf(-c.a * dd);
+        return c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
+    }
+    if (c.kernel == 2) {
+        const float r = sqrtf(dd); const float q = 1.0f / coshf(c.a * r);
+        return c.repulsion_strength * c.a * q * tanhf(c.a * r) / (r * fmaxf(1.0f - q, 1e-3f));
+    }
+    const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
+    return c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
+}
+
+// attraction coefficient at squared distance d2 > 0 (src/layout.cpp:149-157); pw_v = d2^b_uv
+__device__ __forceinline__ float attraction_coeff(const SgdDev& c, float d2, float b_uv, float pw_v) {
+    const float s = -c.exaggeration;
+    if (c.kernel == 0) return s * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
+    if (c.kernel == 1) return s * 2.0f * c.a;
+    if (c.kernel == 2) { const float dd = sqrtf(d2); return s * c.a * tanhf(c.a * dd) / dd; }
+    return s * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
+}
+
+// ---------------------------------------------------------------------------------------------- one sample, in sequence
+// One sampled edge of epoch_worker (src/layout.cpp:136-274), draws in the reference's order from `dr`, n_neg from
+// the schedule. yu: the head's current position (updated in place when it moves); Y: where the other rows are read.
+template <int D, class Sink, class Draws>
+__device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_neg, float alpha, float mid_w,
+                                             Draws& dr, const Sink& sink, const Rec* rec, float* yu, const float* Y) {
     const int dim = D == 0 ? c.dim : D;
     constexpr int DM = D == 0 ? kMaxDim : D;
     const int32_t u = c.head[i], v = c.tail[i];
@@ -147,23 +222,18 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
         d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d]));
         gu[d] = 0.0f;
     }
-    const float b_u = c.node_b ? c.node_b[u] : c.b;
     const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
     const float pw_v = (c.b_is_one && !c.node_b) ? d2 : (d2 > 0.0f ? powf(d2, b_uv) : 0.0f);
+    const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
     int64_t rec_at = rec ? rec->neg_off[i] : 0;
     if (c.loss == 0) {
         if (d2 > 0.0f) {
-            float coeff;
-            const float s = -c.exaggeration;
-            if (c.kernel == 0) coeff = s * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
-            else if (c.kernel == 1) coeff = s * 2.0f * c.a;
-            else if (c.kernel == 2) { const float dd = sqrtf(d2); coeff = s * c.a * tanhf(c.a * dd) / dd; }
-            else coeff = s * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
+            const float coeff = attraction_coeff(c, d2, b_uv, pw_v);
             for (int d = 0; d < dim; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
             if (move_v) sink.template apply<DM>(c, v, gk, alpha, dim);
         }
         for (int p = 0; p < n_neg; ++p) {
-            const int32_t k = (int32_t)rng.below((uint32_t)c.n);
+            const int32_t k = (int32_t)below_of(dr.neg(), (uint32_t)c.n);
             if (rec) { if (rec_at < rec->negs_cap) rec->negs[rec_at] = k; ++rec_at; }
             if (k == u) continue;
             float dd = 0.0f;
@@ -172,26 +242,10 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
                 dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d]));
             }
             if (dd > 0.0f) {
-                float coeff;
-                if (c.kernel == 0) {
-                    if (c.node_b && c.rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f)); }
-                    else { const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b); coeff = c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f)); }
-                } else if (c.kernel == 1) {
-                    const float q = expf(-c.a * dd);
-                    coeff = c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
-                } else if (c.kernel == 2) {
-                    const float r = sqrtf(dd); const float q = 1.0f / coshf(c.a * r);
-                    coeff = c.repulsion_strength * c.a * q * tanhf(c.a * r) / (r * fmaxf(1.0f - q, 1e-3f));
-                } else {
-                    const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
-                    coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
-                }
+                const float coeff = repulsion_coeff(c, dd, u);
                 for (int d = 0; d < dim; ++d) gu[d] += coeff * diff[d];
-            } else if (split_jitter) {
-                Rng jr = jitter_rng(sseed, p);
-                for (int d = 0; d < dim; ++d) gu[d] += (jr.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
             } else {
-                for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                for (int d = 0; d < dim; ++d) gu[d] += (uniform_of(dr.jitter(p, d)) - 0.5f) * jit;
             }
         }
     } else {
@@ -200,7 +254,7 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
         const float q_v = 1.0f / (1.0f + c.a * pw_v);
         float Z = q_v;
         for (int p = 0; p < c.m_neg; ++p) {
-            int32_t k = (int32_t)rng.below((uint32_t)c.n);
+            int32_t k = (int32_t)below_of(dr.neg(), (uint32_t)c.n);
             if (k == u) k = (int32_t)((k + 1) % c.n);
             negs[p] = k;
             if (rec) { if (rec_at < rec->negs_cap) rec->negs[rec_at] = k; ++rec_at; }
@@ -221,12 +275,7 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
             float dd = 0.0f;
             for (int d = 0; d < dim; ++d) { diff[d] = yu[d] - Y[(int64_t)k * dim + d]; dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d])); }
             if (dd <= 0.0f) {
-                if (split_jitter) {
-                    Rng jr = jitter_rng(sseed, p);
-                    for (int d = 0; d < dim; ++d) gu[d] += (jr.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
-                } else {
-                    for (int d = 0; d < dim; ++d) gu[d] += (rng.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
-                }
+                for (int d = 0; d < dim; ++d) gu[d] += (uniform_of(dr.jitter(p, d)) - 0.5f) * jit;
                 continue;
             }
             const float pw = c.b_is_one ? dd : powf(dd, c.b);
@@ -237,30 +286,8 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
         }
     }
     // mid-range partner (src/layout.cpp:225-255)
-    if (mid_w > 0.0f && rng.uniform() < c.mid_rate) {
-        int32_t w = v;
-        if (c.jump_indptr) {
-            const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
-            for (int h = 0; h < L; ++h) {
-                const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
-                if (je > js && rng.uniform() < c.mid_jump) {
-                    w = c.jump_indices[js + (int32_t)rng.below((uint32_t)(je - js))];
-                } else {
-                    const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
-                    if (e0 <= s0) break;
-                    w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
-                }
-            }
-        } else if (c.mid_pairs) {
-            w = c.mid_pairs[(int64_t)u * c.n_mid + rng.below((uint32_t)c.n_mid)];
-        } else {
-            const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
-            for (int h = 0; h < L; ++h) {
-                const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
-                if (e0 <= s0) break;
-                w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
-            }
-        }
+    if (mid_w > 0.0f && uniform_of(dr.mid()) < c.mid_rate) {
+        const int32_t w = mid_partner(c, u, v, dr);
         if (rec) rec->mid[i] = (w != u) ? w : -2;
         if (w != u) {
             for (int d = 0; d < dim; ++d) {
@@ -273,8 +300,8 @@ __device__ __forceinline__ void process_edge(const SgdDev& c, int64_t i, int n_n
     if (move_u) local_step<DM>(c, yu, gu, alpha, u, dim);
 }
 
-// Schedule of one sample (src/layout.cpp:135, 160-163, 184; InfoNCE :221-222): returns n_neg or -1 when the
-// edge is not sampled this epoch, and advances eons / eonns.
+// Schedule of one sample (src/layout.cpp:135, 160-163, 184; InfoNCE :221-222): n_neg, or -1 when the edge is not
+// sampled this epoch; advances eons / eonns.
 __device__ __forceinline__ int schedule_edge(const SgdDev& c, int64_t i, float fepoch) {
     const float eon = c.eons[i];
     if (eon > fepoch) return -1;
@@ -291,7 +318,6 @@ __device__ __forceinline__ int schedule_edge(const SgdDev& c, int64_t i, float f
     return c.m_neg;
 }
 
-// ---------------------------------------------------------------------------------------------- kernels
 template <int D>
 __device__ __forceinline__ void load_row(const float* Y, int64_t u, int dim, float* yu) {
 #pragma unroll
@@ -299,10 +325,161 @@ __device__ __forceinline__ void load_row(const float* Y, int64_t u, int dim, flo
         if (d < dim) yu[d] = Y[u * dim + d];
 }
 
-// Row kernel, hogwild: one thread owns head u and walks its edges in order (edges sorted by head, row pointers
-// eptr). The head's steps accumulate in registers one after another, as in the reference's loop; the tail,
-// mid-range partner (and InfoNCE negatives) move through float atomics. The head's total displacement lands with
-// one atomic at the end, on top of whatever the other rows added to it meanwhile.
+// the head's whole displacement of the row, on top of what the other rows added to it meanwhile
+template <int D>
+__device__ __forceinline__ void flush_head(const SgdDev& c, int64_t u, int dim, const float* yu, const float* y0) {
+    if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
+    else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
+}
+
+// ---------------------------------------------------------------------------------------------- counter mode kernels
+constexpr int kGroup = 8;
+constexpr int kNegPerRound = kGroup - 2;
+
+__device__ __forceinline__ float group_sum(float v, unsigned gmask) {
+#pragma unroll
+    for (int o = kGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o, kGroup);
+    return v;
+}
+
+// Warp kernel, loss 0, dim 2 or 3, edges sorted by head. A warp carries 4 groups of 8 lanes; each group owns one
+// head row at a time and the 4 groups advance in lockstep, one sample each per iteration. Within a sample every
+// lane runs the same code on one interaction: lanes 0-5 the negatives (negative p on lane p mod 6, in rounds when
+// there are more than 6), lane 6 the attraction towards the tail, lane 7 the mid-range partner. The head's
+// gradient is the group sum and its step is applied before the group's next sample, as in the reference's loop;
+// the tail and the partner take their steps through float2 atomics; the head's whole displacement lands with one
+// atomic when the group leaves the row.
+template <int D>
+__global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+                                                                 int epoch, float alpha, float mid_w) {
+    const int lane = threadIdx.x & 31;
+    const int gl = lane & (kGroup - 1);
+    const int gbase = lane & ~(kGroup - 1);
+    const unsigned gmask = ((1u << kGroup) - 1u) << gbase;
+    const float fepoch = (float)epoch;
+    const int64_t n_groups = (int64_t)gridDim.x * (blockDim.x / kGroup);
+    const int role = gl < kNegPerRound ? 0 : (gl == kNegPerRound ? 1 : 2);   // negative / attraction / mid-range
+    const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
+    // the common coefficient path: kernel 0 without per-node b, one powf per lane
+    const bool uniform_path = c.kernel == 0 && !c.node_b;
+    const float ex = role == 1 ? c.b : c.rep_b;
+    const bool plain = role == 1 ? c.b_is_one : c.rep_b_is_one;
+    int64_t u = (int64_t)blockIdx.x * (blockDim.x / kGroup) + threadIdx.x / kGroup;
+    int64_t e1 = 0, base = 0;
+    unsigned sm = 0;
+    int nn = -1;
+    float yu[D], y0[D];
+    bool have = false;
+    if (u < c.n) { base = eptr[u] - kGroup; e1 = eptr[u + 1]; }
+    for (;;) {
+        // ---- each group moves to its next sampled edge (group-uniform control flow)
+        while (u < c.n && sm == 0) {
+            base += kGroup;
+            if (base >= e1) {
+                if (have && gl == 0 && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+                have = false;
+                u += n_groups;
+                if (u < c.n) { base = eptr[u] - kGroup; e1 = eptr[u + 1]; }
+                continue;
+            }
+            const int64_t i = base + gl;
+            nn = i < e1 ? schedule_edge(c, i, fepoch) : -1;
+            sm = (__ballot_sync(gmask, nn >= 0) >> gbase) & ((1u << kGroup) - 1u);
+        }
+        const bool active = u < c.n;
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
+        // ---- one sample of the group
+        const int src = __ffs(sm) - 1;
+        sm &= sm - 1;
+        const int n_neg = __shfl_sync(gmask, nn, src, kGroup);
+        const int64_t i = base + src;
+        if (!have) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) { yu[d] = c.Y[u * D + d]; y0[d] = yu[d]; }
+            have = true;
+        }
+        const int32_t v = c.tail[i];
+        const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
+        float gu[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) gu[d] = 0.0f;
+        const int rounds = n_neg > kNegPerRound ? (n_neg + kNegPerRound - 1) / kNegPerRound : 1;
+        for (int r = 0; r < rounds; ++r) {
+            const int p = r * kNegPerRound + gl;
+            // this lane's partner row, or -1 when it has none this round
+            int32_t partner = -1;
+            if (role == 0) {
+                if (p < n_neg) {
+                    const int32_t k = (int32_t)below_of(counter_draw(ss, p), (uint32_t)c.n);
+                    partner = k == (int32_t)u ? -1 : k;
+                }
+            } else if (r == 0) {
+                if (role == 1) {
+                    partner = v;
+                } else if (mid_w > 0.0f) {
+                    CounterDraws dr(ss);
+                    if (uniform_of(dr.mid()) < c.mid_rate) {
+                        const int32_t w = mid_partner(c, (int32_t)u, v, dr);
+                        partner = w == (int32_t)u ? -1 : w;
+                    }
+                }
+            }
+            if (partner >= 0) {
+                float diff[D], d2 = 0.0f;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    diff[d] = yu[d] - c.Y[(int64_t)partner * D + d];
+                    d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d]));
+                }
+                const bool pos = d2 > 0.0f;
+                float coeff;
+                if (uniform_path) {
+                    const float pw = (plain || !pos) ? d2 : powf(d2, ex);
+                    const float att = -c.exaggeration * 2.0f * c.a * c.b * pw / (d2 * (c.a * pw + 1.0f));
+                    const float rep = c.two_b / ((0.001f + d2) * (c.rep_a * pw + 1.0f));
+                    coeff = role == 0 ? rep : (role == 1 ? att : -mid_w);
+                } else if (role == 0) {
+                    coeff = pos ? repulsion_coeff(c, d2, (int32_t)u) : 0.0f;
+                } else if (role == 1) {
+                    const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
+                    const float pw_v = (c.b_is_one && !c.node_b) ? d2 : (pos ? powf(d2, b_uv) : 0.0f);
+                    coeff = pos ? attraction_coeff(c, d2, b_uv, pw_v) : 0.0f;
+                } else {
+                    coeff = -mid_w;
+                }
+                if (!pos && role != 2) coeff = 0.0f;
+                float gk[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
+                if (role == 0 && !pos) {
+#pragma unroll
+                    for (int d = 0; d < D; ++d)
+                        gu[d] += (uniform_of(counter_draw(ss, kJitterDraw + 64 * p + d)) - 0.5f) * jit;
+                }
+                const bool moves = ((role == 1 && pos) || role == 2) && partner >= c.n_fixed;
+                if (moves) HogwildSink().template apply<D>(c, partner, gk, alpha, D);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) gu[d] = group_sum(gu[d], gmask);
+        if (u >= c.n_fixed) {
+            float step[D];
+            if (c.optimizer == 1) {
+                // lazy Adam of the head: one lane updates the state, the step is broadcast
+                if (gl == 0) make_step<D>(c, gu, alpha, u, D, step);
+#pragma unroll
+                for (int d = 0; d < D; ++d) step[d] = __shfl_sync(gmask, step[d], 0, kGroup);
+            } else {
+                make_step<D>(c, gu, alpha, u, D, step);
+            }
+#pragma unroll
+            for (int d = 0; d < D; ++d) yu[d] += step[d];
+        }
+    }
+}
+
+// Row kernel (any dim, any loss): one thread owns a head row and walks it in order with counter draws.
 template <int D>
 __global__ void __launch_bounds__(kThreads) hogwild_rows_kernel(SgdDev c, const int64_t* __restrict__ eptr, int epoch,
                                                                 float alpha, float mid_w) {
@@ -311,198 +488,20 @@ __global__ void __launch_bounds__(kThreads) hogwild_rows_kernel(SgdDev c, const 
     const float fepoch = (float)epoch;
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < c.n; u += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e0 = eptr[u], e1 = eptr[u + 1];
-        if (e0 == e1) continue;
         float yu[DM], y0[DM];
         bool any = false;
         for (int64_t i = e0; i < e1; ++i) {
             const int n_neg = schedule_edge(c, i, fepoch);
             if (n_neg < 0) continue;
             if (!any) { load_row<D>(c.Y, u, dim, yu); for (int d = 0; d < dim; ++d) y0[d] = yu[d]; any = true; }
-            const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
-            Rng rng(ss);
-            process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y, true, ss);
+            CounterDraws dr(stream_seed(c.seed, epoch, (uint64_t)i));
+            process_edge<D>(c, i, n_neg, alpha, mid_w, dr, HogwildSink(), nullptr, yu, c.Y);
         }
-        if (!any || u < c.n_fixed) continue;
-        if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
-        else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
+        if (any && u >= c.n_fixed) flush_head<D>(c, u, dim, yu, y0);
     }
 }
 
-
-// Group kernel, hogwild, loss 0, dim 2 or 3: kGroup lanes own one head row. They read the row's schedule in
-// coalesced chunks of kGroup edges and ballot the sampled ones; each sample is then processed by the whole group:
-// negative p on lane p % (kGroup - 2) (lane p draws the p-th value of the edge's stream directly), the mid-range
-// partner on lane kGroup - 2, the attraction on lane kGroup - 1; the head's gradient is the group sum, and the
-// head's step is applied before the next sample, as in the reference's loop. Tails and partners move through
-// float2 atomics; the head's total displacement lands with one atomic at the end of the row.
-constexpr int kGroup = 8;
-
-template <int D>
-__device__ __forceinline__ float group_sum(float v, unsigned gmask) {
-#pragma unroll
-    for (int o = kGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o, kGroup);
-    return v;
-}
-
-template <int D>
-__device__ __forceinline__ void group_sample(const SgdDev& c, int64_t i, int32_t u, int n_neg, float alpha, float mid_w,
-                                             int epoch, int gl, unsigned gmask, float* yu) {
-    const int32_t v = c.tail[i];
-    const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
-    float gu[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) gu[d] = 0.0f;
-    constexpr int kNegLanes = kGroup - 2;
-    if (gl == kGroup - 1) {
-        // attraction (src/layout.cpp:149-159)
-        float diff[D], d2 = 0.0f;
-#pragma unroll
-        for (int d = 0; d < D; ++d) { diff[d] = yu[d] - c.Y[(int64_t)v * D + d]; d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d])); }
-        if (d2 > 0.0f) {
-            const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
-            const float pw_v = (c.b_is_one && !c.node_b) ? d2 : powf(d2, b_uv);
-            const float s = -c.exaggeration;
-            float coeff;
-            if (c.kernel == 0) coeff = s * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
-            else if (c.kernel == 1) coeff = s * 2.0f * c.a;
-            else if (c.kernel == 2) { const float dd = sqrtf(d2); coeff = s * c.a * tanhf(c.a * dd) / dd; }
-            else coeff = s * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
-            float gk[D];
-#pragma unroll
-            for (int d = 0; d < D; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
-            if (v >= c.n_fixed) HogwildSink().template apply<D>(c, v, gk, alpha, D);
-        }
-    } else if (gl == kGroup - 2) {
-        // mid-range partner (src/layout.cpp:225-255): draws n_neg and on of the stream
-        if (mid_w > 0.0f) {
-            Rng rng(ss);
-            for (int p = 0; p < n_neg; ++p) rng.next();
-            if (rng.uniform() < c.mid_rate) {
-                int32_t w = v;
-                if (c.jump_indptr) {
-                    const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
-                    for (int h = 0; h < L; ++h) {
-                        const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
-                        if (je > js && rng.uniform() < c.mid_jump) {
-                            w = c.jump_indices[js + (int32_t)rng.below((uint32_t)(je - js))];
-                        } else {
-                            const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
-                            if (e0 <= s0) break;
-                            w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
-                        }
-                    }
-                } else if (c.mid_pairs) {
-                    w = c.mid_pairs[(int64_t)u * c.n_mid + rng.below((uint32_t)c.n_mid)];
-                } else {
-                    const int L = c.walk_lens ? c.walk_lens[v] : c.walk_len;
-                    for (int h = 0; h < L; ++h) {
-                        const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
-                        if (e0 <= s0) break;
-                        w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
-                    }
-                }
-                if (w != u) {
-                    float gk[D];
-#pragma unroll
-                    for (int d = 0; d < D; ++d) {
-                        const float g = -mid_w * (yu[d] - c.Y[(int64_t)w * D + d]);
-                        gu[d] += g; gk[d] = -g;
-                    }
-                    if (w >= c.n_fixed) HogwildSink().template apply<D>(c, w, gk, alpha, D);
-                }
-            }
-        }
-    }
-    // negatives (src/layout.cpp:164-183), negative p on lane p % kNegLanes
-    if (gl < kNegLanes && gl < n_neg) {
-        Rng rng(ss);
-        for (int p = 0; p < gl; ++p) rng.next();
-        const float b_u = c.node_b ? c.node_b[u] : c.b;
-        for (int p = gl; p < n_neg; p += kNegLanes) {
-            const int32_t k = (int32_t)rng.below((uint32_t)c.n);
-            for (int q = 1; q < kNegLanes; ++q) rng.next();
-            if (k == u) continue;
-            float diff[D], dd = 0.0f;
-#pragma unroll
-            for (int d = 0; d < D; ++d) { diff[d] = yu[d] - c.Y[(int64_t)k * D + d]; dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d])); }
-            if (dd > 0.0f) {
-                float coeff;
-                if (c.kernel == 0) {
-                    if (c.node_b && c.rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f)); }
-                    else { const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b); coeff = c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f)); }
-                } else if (c.kernel == 1) {
-                    const float q = expf(-c.a * dd);
-                    coeff = c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
-                } else if (c.kernel == 2) {
-                    const float r = sqrtf(dd); const float q = 1.0f / coshf(c.a * r);
-                    coeff = c.repulsion_strength * c.a * q * tanhf(c.a * r) / (r * fmaxf(1.0f - q, 1e-3f));
-                } else {
-                    const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
-                    coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
-                }
-#pragma unroll
-                for (int d = 0; d < D; ++d) gu[d] += coeff * diff[d];
-            } else {
-                Rng jr = jitter_rng(ss, p);
-#pragma unroll
-                for (int d = 0; d < D; ++d) gu[d] += (jr.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
-            }
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < D; ++d) gu[d] = group_sum<D>(gu[d], gmask);
-    if (u >= c.n_fixed) {
-        float step[D];
-        if (c.optimizer == 1) {
-            // lazy Adam of the head: one lane updates the state, the step is broadcast
-            if (gl == 0) make_step<D>(c, gu, alpha, u, D, step);
-#pragma unroll
-            for (int d = 0; d < D; ++d) step[d] = __shfl_sync(gmask, step[d], 0, kGroup);
-        } else {
-            make_step<D>(c, gu, alpha, u, D, step);
-        }
-#pragma unroll
-        for (int d = 0; d < D; ++d) yu[d] += step[d];
-    }
-}
-
-template <int D>
-__global__ void __launch_bounds__(kThreads) hogwild_groups_kernel(SgdDev c, const int64_t* __restrict__ eptr,
-                                                                  int epoch, float alpha, float mid_w) {
-    const int lane = threadIdx.x & 31;
-    const int gl = lane & (kGroup - 1);
-    const int gbase = lane & ~(kGroup - 1);
-    const unsigned gmask = ((1u << kGroup) - 1u) << gbase;
-    const float fepoch = (float)epoch;
-    const int64_t groups = (int64_t)gridDim.x * (blockDim.x / kGroup);
-    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x / kGroup) + threadIdx.x / kGroup; u < c.n; u += groups) {
-        const int64_t e0 = eptr[u], e1 = eptr[u + 1];
-        float yu[D], y0[D];
-        bool have = false;
-        for (int64_t base = e0; base < e1; base += kGroup) {
-            const int64_t i = base + gl;
-            const int nn = i < e1 ? schedule_edge(c, i, fepoch) : -1;
-            unsigned sm = (__ballot_sync(gmask, nn >= 0) >> gbase) & ((1u << kGroup) - 1u);
-            while (sm) {
-                const int src = __ffs(sm) - 1;
-                sm &= sm - 1;
-                const int n_neg = __shfl_sync(gmask, nn, src, kGroup);
-                if (!have) {
-#pragma unroll
-                    for (int d = 0; d < D; ++d) { yu[d] = c.Y[u * D + d]; y0[d] = yu[d]; }
-                    have = true;
-                }
-                group_sample<D>(c, base + src, (int32_t)u, n_neg, alpha, mid_w, epoch, gl, gmask, yu);
-            }
-        }
-        if (have && gl == 0 && u >= c.n_fixed) {
-            if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
-            else for (int d = 0; d < D; ++d) atomicAdd(&c.Y[u * D + d], yu[d] - y0[d]);
-        }
-    }
-}
-
-// Edge kernel, hogwild (edges not sorted by head): one thread per edge; the head's step lands with an atomic.
+// Edge kernel (edges not sorted by head): one thread per edge; the head's step lands with an atomic.
 template <int D>
 __global__ void __launch_bounds__(kThreads) hogwild_edges_kernel(SgdDev c, int epoch, float alpha, float mid_w) {
     const int dim = D == 0 ? c.dim : D;
@@ -515,68 +514,40 @@ __global__ void __launch_bounds__(kThreads) hogwild_edges_kernel(SgdDev c, int e
         float yu[DM], y0[DM];
         load_row<D>(c.Y, u, dim, yu);
         for (int d = 0; d < dim; ++d) y0[d] = yu[d];
-        const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
-        Rng rng(ss);
-        process_edge<D>(c, i, n_neg, alpha, mid_w, rng, HogwildSink(), nullptr, yu, c.Y, true, ss);
-        if (u < c.n_fixed) continue;
-        if (D == 2) atomicAdd(reinterpret_cast<float2*>(c.Y) + u, make_float2(yu[0] - y0[0], yu[1] - y0[1]));
-        else for (int d = 0; d < dim; ++d) atomicAdd(&c.Y[u * dim + d], yu[d] - y0[d]);
+        CounterDraws dr(stream_seed(c.seed, epoch, (uint64_t)i));
+        process_edge<D>(c, i, n_neg, alpha, mid_w, dr, HogwildSink(), nullptr, yu, c.Y);
+        if (u >= c.n_fixed) flush_head<D>(c, u, dim, yu, y0);
     }
 }
 
-// serial stream, phase 1: the schedule of the epoch (parallel); cnt[i] = n_neg or -1
+// ---------------------------------------------------------------------------------------------- serial mode kernels
+// phase 1: the schedule of the epoch (parallel); cnt[i] = n_neg or -1
 __global__ void serial_schedule_kernel(SgdDev c, int epoch, int32_t* __restrict__ cnt) {
     const float fepoch = (float)epoch;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges; i += (int64_t)gridDim.x * blockDim.x)
         cnt[i] = schedule_edge(c, i, fepoch);
 }
 
-// serial stream, phase 2: one thread walks the sampled edges in order through the epoch's single stream
-// (seed tid 0) and records the generator state at the start of each sampled edge. It consumes the draws of
-// each sample as the reference does: n_neg (or m_neg) below() calls, then with a mid weight one uniform() and,
-// on success, the partner draws (a pair index, or the steps of the walk).
+// phase 2: one thread walks the sampled edges in order through the epoch's single stream (seed tid 0) and records
+// the generator state at the start of each sampled edge, consuming the draws of each sample as the reference does:
+// n_neg (or m_neg) below() calls, then with a mid-range weight one uniform() and, on success, the partner draws.
 __global__ void serial_chain_kernel(SgdDev c, int epoch, float mid_w, const int32_t* __restrict__ cnt,
                                     uint64_t* __restrict__ state) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    Rng rng(stream_seed(c.seed, epoch, 0));
+    SerialDraws dr{Rng(stream_seed(c.seed, epoch, 0))};
     for (int64_t i = 0; i < c.n_edges; ++i) {
         const int k = cnt[i];
         if (k < 0) continue;
-        state[i] = rng.s;
-        for (int p = 0; p < k; ++p) rng.next();
-        if (mid_w > 0.0f && rng.uniform() < c.mid_rate) {
-            int32_t w = c.tail[i];
-            if (c.jump_indptr) {
-                const int L = c.walk_lens ? c.walk_lens[c.tail[i]] : c.walk_len;
-                for (int h = 0; h < L; ++h) {
-                    const int32_t js = c.jump_indptr[w], je = c.jump_indptr[w + 1];
-                    if (je > js && rng.uniform() < c.mid_jump) {
-                        w = c.jump_indices[js + (int32_t)rng.below((uint32_t)(je - js))];
-                    } else {
-                        const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
-                        if (e0 <= s0) break;
-                        w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
-                    }
-                }
-            } else if (c.mid_pairs) {
-                rng.next();
-            } else {
-                const int L = c.walk_lens ? c.walk_lens[c.tail[i]] : c.walk_len;
-                for (int h = 0; h < L; ++h) {
-                    const int32_t s0 = c.indptr[w], e0 = c.indptr[w + 1];
-                    if (e0 <= s0) break;
-                    w = c.indices[s0 + (int32_t)rng.below((uint32_t)(e0 - s0))];
-                }
-            }
-        }
+        state[i] = dr.r.s;
+        for (int p = 0; p < k; ++p) dr.r.next();
+        if (mid_w > 0.0f && uniform_of(dr.mid()) < c.mid_rate) mid_partner(c, c.head[i], c.tail[i], dr);
     }
 }
 
-// serial stream, phase 3 (rows), in kSerialPhases sub-steps: sub-step p processes the p-th sampled edge of every
-// head row (the last sub-step the rest of the row, in order) from its recorded state, reading every position as
-// committed after the previous sub-step; the displacements of the sub-step are summed in fixed point and
-// committed before the next one. Each sub-step's result is a function of its inputs only, and the reads are
-// never older than one sub-step (about one edge sample per head) instead of one epoch.
+// phase 3 (rows), in kSerialPhases sub-steps: sub-step p processes the p-th sampled edge of every head row (the
+// last sub-step the rest of the row, in order) from its recorded state, reading every position as committed after
+// the previous sub-step; the sub-step's displacements are summed in fixed point and committed before the next.
+// Each sub-step's result is a function of its inputs only, and the reads are never older than one sub-step.
 constexpr int kSerialPhases = 8;
 
 template <int D>
@@ -600,9 +571,9 @@ __global__ void __launch_bounds__(kThreads) serial_rows_kernel(SgdDev c, const i
             const int idx = seen++;
             if (idx < phase) continue;
             if (!any) { load_row<D>(c.Y, u, dim, yu); for (int d = 0; d < dim; ++d) y0[d] = yu[d]; any = true; }
-            Rng rng(0);
-            rng.s = state[i];
-            process_edge<D>(c, i, k, alpha, mid_w, rng, sink, nullptr, yu, c.Y);
+            SerialDraws dr{Rng(0)};
+            dr.r.s = state[i];
+            process_edge<D>(c, i, k, alpha, mid_w, dr, sink, nullptr, yu, c.Y);
             if (!last) break;
         }
         if (!any || u < c.n_fixed) continue;
@@ -611,10 +582,9 @@ __global__ void __launch_bounds__(kThreads) serial_rows_kernel(SgdDev c, const i
     }
 }
 
-// serial stream, phase 3 (edges not sorted by head): one thread per sampled edge against the snapshot
+// phase 3 (edges not sorted by head): one thread per sampled edge against the epoch-start layout
 template <int D>
-__global__ void __launch_bounds__(kThreads) serial_edges_kernel(SgdDev c, const float* __restrict__ Ysnap,
-                                                                float alpha, float mid_w,
+__global__ void __launch_bounds__(kThreads) serial_edges_kernel(SgdDev c, float alpha, float mid_w,
                                                                 const int32_t* __restrict__ cnt,
                                                                 const uint64_t* __restrict__ state,
                                                                 unsigned long long* __restrict__ delta) {
@@ -626,18 +596,18 @@ __global__ void __launch_bounds__(kThreads) serial_edges_kernel(SgdDev c, const 
         if (k < 0) continue;
         const int64_t u = c.head[i];
         float yu[DM], y0[DM];
-        load_row<D>(Ysnap, u, dim, yu);
+        load_row<D>(c.Y, u, dim, yu);
         for (int d = 0; d < dim; ++d) y0[d] = yu[d];
-        Rng rng(0);
-        rng.s = state[i];
-        process_edge<D>(c, i, k, alpha, mid_w, rng, sink, nullptr, yu, Ysnap);
+        SerialDraws dr{Rng(0)};
+        dr.r.s = state[i];
+        process_edge<D>(c, i, k, alpha, mid_w, dr, sink, nullptr, yu, c.Y);
         if (u < c.n_fixed) continue;
         for (int d = 0; d < dim; ++d)
             atomicAdd(&delta[u * dim + d], (unsigned long long)llrint((double)(yu[d] - y0[d]) * kFix));
     }
 }
 
-// serial stream, phase 4: y = snapshot + delta * 2^-32 (the snapshot is the layout itself), delta = 0
+// phase 4: y += delta * 2^-32, delta = 0
 __global__ void commit_kernel(float* __restrict__ Y, unsigned long long* __restrict__ delta, int64_t total) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
         const long long q = (long long)delta[k];
@@ -648,6 +618,7 @@ __global__ void commit_kernel(float* __restrict__ Y, unsigned long long* __restr
     }
 }
 
+// ---------------------------------------------------------------------------------------------- helpers
 // row pointers of an edge list sorted by head: eptr[u] = first edge with head >= u
 __global__ void row_ptr_kernel(const int32_t* __restrict__ head, int64_t E, int64_t n, int64_t* __restrict__ eptr) {
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u <= n; u += (int64_t)gridDim.x * blockDim.x) {
@@ -675,13 +646,16 @@ __global__ void record_kernel(SgdDev c, int epoch, float alpha, float mid_w, con
         rec.mid[i] = -1;
         const int k = cnt[i];
         if (k < 0) continue;
-        Rng rng(0);
-        const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
-        if (per_edge) rng = Rng(ss);
-        else rng.s = state[i];
         float yu[DM];
         load_row<D>(c.Y, c.head[i], dim, yu);
-        process_edge<D>(c, i, k, alpha, mid_w, rng, NullSink(), &rec, yu, c.Y, per_edge != 0, ss);
+        if (per_edge) {
+            CounterDraws dr(stream_seed(c.seed, epoch, (uint64_t)i));
+            process_edge<D>(c, i, k, alpha, mid_w, dr, NullSink(), &rec, yu, c.Y);
+        } else {
+            SerialDraws dr{Rng(0)};
+            dr.r.s = state[i];
+            process_edge<D>(c, i, k, alpha, mid_w, dr, NullSink(), &rec, yu, c.Y);
+        }
     }
 }
 
@@ -719,16 +693,17 @@ __global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64
 template <int D>
 void hogwild_epoch(const SgdDev& c, const int64_t* eptr, int epoch, float alpha, float mid_w, cudaStream_t s) {
     if (eptr && c.loss == 0 && (D == 2 || D == 3))
-        hogwild_groups_kernel<D == 0 ? 2 : D><<<blocks_for(c.n, kThreads / kGroup), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
+        hogwild_warps_kernel<D == 0 ? 2 : D><<<blocks_for(c.n, kThreads / kGroup, 8), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
     else if (eptr) hogwild_rows_kernel<D><<<blocks_for(c.n, kThreads), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
     else hogwild_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, alpha, mid_w);
 }
+
 template <int D>
 void serial_apply(const SgdDev& c, const int64_t* eptr, float alpha, float mid_w, const int32_t* cnt,
                   const uint64_t* st, unsigned long long* delta, cudaStream_t s) {
     const int64_t total = c.n * c.dim;
     if (!eptr) {
-        serial_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, c.Y, alpha, mid_w, cnt, st, delta);
+        serial_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, alpha, mid_w, cnt, st, delta);
         MGB_LAUNCH_CHECK();
         commit_kernel<<<blocks_for(total, kThreads), kThreads, 0, s>>>(c.Y, delta, total);
         return;
@@ -740,6 +715,7 @@ void serial_apply(const SgdDev& c, const int64_t* eptr, float alpha, float mid_w
         if (p + 1 < kSerialPhases) MGB_LAUNCH_CHECK();
     }
 }
+
 template <int D>
 void record_launch(const SgdDev& c, int epoch, float alpha, float mid_w, const int32_t* cnt, const uint64_t* st,
                    int per_edge, Rec rec, cudaStream_t s) {
@@ -753,8 +729,7 @@ void record_launch(const SgdDev& c, int epoch, float alpha, float mid_w, const i
         default: F<0>(__VA_ARGS__); break;           \
     }
 
-// row pointers when the edges are sorted by head (the reference's schedule is the COO of a sorted CSR), else
-// nullptr (edge-parallel kernels)
+// row pointers when the edges are sorted by head, else nullptr (edge-parallel kernels)
 const int64_t* row_pointers(const SgdDev& c, SgdWork& w, cudaStream_t s) {
     if (c.n_edges == 0) return nullptr;
     int* flag = static_cast<int*>(w.flag.ensure(sizeof(int)));

@@ -336,43 +336,56 @@ __global__ void mid_spring_kernel(const float* __restrict__ Y, const int32_t* __
     }
 }
 
-// column means (FP64) subtracted, then column 0's standard deviation (FP64, population) brought to target
-__global__ void center_scale_kernel(float* __restrict__ Y, int64_t n, int dim, double target) {
-    __shared__ double red[kThreads / 32];
-    __shared__ float mean_f[kMaxDim];
-    __shared__ float factor;
-    for (int d = 0; d < dim; ++d) {
+// The hybrid hand-off in two grid-wide passes: FP64 partial sums of every column and of column 0's squares per
+// block, the last block turning them into the means and the scale factor target / std(Y[:, 0]); then
+// Y = (Y - mean) * factor.
+__global__ void __launch_bounds__(kThreads) center_stats_kernel(const float* __restrict__ Y, int64_t n, int dim,
+                                                                double target, double* __restrict__ part,
+                                                                unsigned* __restrict__ counter, float* __restrict__ out) {
+    __shared__ double red[kThreads / 32][kMaxDim + 1];
+    __shared__ int is_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 0; d <= dim; ++d) {
         double s = 0.0;
-        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += (double)Y[i * dim + d];
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            const double v = (double)Y[i * dim + (d < dim ? d : 0)];
+            s += d < dim ? v : v * v;
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-            mean_f[d] = (float)(t / (double)n);
-        }
-        __syncthreads();
+        if (lane == 0) red[warp][d] = s;
     }
-    for (int64_t k = threadIdx.x; k < n * dim; k += blockDim.x) Y[k] -= mean_f[k % dim];
     __syncthreads();
-    double s = 0.0, s2 = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) { const double v = Y[i * dim]; s += v; s2 += v * v; }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); s2 += __shfl_xor_sync(0xffffffffu, s2, o); }
-    __shared__ double red2[kThreads / 32];
-    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; red2[threadIdx.x >> 5] = s2; }
+    if (threadIdx.x <= dim) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+        part[(size_t)blockIdx.x * (kMaxDim + 1) + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    if (threadIdx.x <= dim) {
+        double t = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) t += __ldcg(&part[(size_t)b * (kMaxDim + 1) + threadIdx.x]);
+        red[0][threadIdx.x] = t;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0, t2 = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { t += red[w]; t2 += red2[w]; }
-        const double m = t / (double)n;
-        const double sd = sqrt(fmax(t2 / (double)n - m * m, 0.0));
-        factor = (float)(target / fmax(sd, 1e-12));
+        for (int d = 0; d < dim; ++d) out[d] = (float)(red[0][d] / (double)n);
+        const double m0 = red[0][0] / (double)n;
+        const double var = fmax(red[0][dim] / (double)n - m0 * m0, 0.0);
+        out[kMaxDim] = (float)(target / fmax(sqrt(var), 1e-12));
+        *counter = 0u;
     }
-    __syncthreads();
-    for (int64_t k = threadIdx.x; k < n * dim; k += blockDim.x) Y[k] *= factor;
+}
+
+__global__ void center_apply_kernel(float* __restrict__ Y, int64_t total, int dim, const float* __restrict__ st) {
+    const float f = st[kMaxDim];
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x)
+        Y[k] = (Y[k] - st[k % dim]) * f;
 }
 
 __global__ void init_opt_state_kernel(float2* U, float2* G, int64_t n) {
@@ -449,9 +462,18 @@ void mid_spring_dev(const float* Y, const int32_t* pairs, float* grad, int64_t n
     MGB_LAUNCH_CHECK();
 }
 
-void center_scale_dev(float* Y, int64_t n, int dim, double target_std, DevBuf&, cudaStream_t s) {
+void center_scale_dev(float* Y, int64_t n, int dim, double target_std, DevBuf& scratch, cudaStream_t s) {
     if (n == 0) return;
-    center_scale_kernel<<<1, kThreads, 0, s>>>(Y, n, dim, target_std);
+    const int blocks = grid_blocks(n, kThreads, 4);
+    // layout of the scratch: counter at 0, means + factor at 64, per-block partials at 1024
+    char* base = static_cast<char*>(scratch.ensure(1024 + sizeof(double) * (kMaxDim + 1) * blocks));
+    unsigned* counter = reinterpret_cast<unsigned*>(base);
+    float* st = reinterpret_cast<float*>(base + 64);
+    double* part = reinterpret_cast<double*>(base + 1024);
+    MGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
+    center_stats_kernel<<<blocks, kThreads, 0, s>>>(Y, n, dim, target_std, part, counter, st);
+    MGB_LAUNCH_CHECK();
+    center_apply_kernel<<<grid_blocks(n * dim, kThreads, 8), kThreads, 0, s>>>(Y, n * dim, dim, st);
     MGB_LAUNCH_CHECK();
 }
 

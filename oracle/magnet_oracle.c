@@ -12,9 +12,8 @@
  *   orc_sgd_serial      src/layout.cpp:90-116 (apply_step), :118-276 (epoch_worker, hogwild path),
  *                       :281-297 (run_epochs, single-thread path), :343-472 (optimize_layout argument rules)
  *   orc_sgd_schedule    the draws epoch_worker makes (src/layout.cpp:123,135,160-166,184,226-249), recorded
- *                       instead of applied; one stream per epoch (tid 0, the n_threads=1 reference), or one
- *                       stream per edge (the device's fast mode: the reference's seeding formula with tid = edge
- *                       index, and the distance-0 jitter drawn from a side stream per negative)
+ *                       instead of applied; one stream per epoch (tid 0, the n_threads=1 reference), or the
+ *                       device fast mode's counter draws (each draw of a sample addressed by edge and index)
  *   orc_spread / orc_gather  src/fftconv.cpp:24-40 (lagrange_w), :83-123 (spread), :200-229 (gather)
  *   orc_tsne_attraction src/fftrep.cpp:129-177
  *   orc_tsne_step       src/fftrep.cpp:225-266 (one thread: nt = 1 partial sums, i.e. blocks of 1024 rows)
@@ -55,10 +54,26 @@ static inline uint64_t orc_stream_seed(uint64_t seed, int epoch, uint64_t tid) {
     return seed * 0x9E3779B1ULL + (uint64_t)epoch * 0x85EBCA6BULL + tid * 0xC2B2AE35ULL;
 }
 
-/* per-edge stream mode: the distance-0 jitter of negative p comes from a side stream (the device's
- * jitter_rng), so that the main stream holds only the negatives, the mid-range draw and the partner draws */
-static void orc_jitter_seed(orc_rng* r, uint64_t sseed, int p) {
-    orc_rng_seed(r, sseed ^ 0xA24BAED4963EE407ULL ^ ((uint64_t)(p + 1) * 0x9FB21C651E98DF25ULL));
+/* Draw sources of one sample. Serial: the epoch's single stream, consumed in order (the reference).
+ * Counter (the device's fast mode): draw j of edge i in epoch e is the first output of the generator seeded with
+ * orc_stream_seed(seed, e, i) ^ (j * 0x9E3779B97F4A7C15); negative p is draw p, the mid-range draws are draws
+ * 1024, 1025, ..., and the distance-0 jitter of negative p in dimension q is draw 2048 + 64 p + q. */
+typedef struct { orc_rng rng; int counter; uint64_t ss; int p, t; } orc_draws;
+
+static inline uint64_t orc_counter_draw(uint64_t ss, int j) {
+    orc_rng r; orc_rng_seed(&r, ss ^ ((uint64_t)j * 0x9E3779B97F4A7C15ULL));
+    return orc_rng_next(&r);
+}
+static inline uint32_t orc_below_of(uint64_t x, uint32_t n) { return (uint32_t)(((x >> 32) * (uint64_t)n) >> 32); }
+static inline float orc_uniform_of(uint64_t x) { return (float)(x >> 40) * (1.0f / 16777216.0f); }
+static inline uint64_t orc_draw_neg(orc_draws* d) {
+    return d->counter ? orc_counter_draw(d->ss, d->p++) : orc_rng_next(&d->rng);
+}
+static inline uint64_t orc_draw_mid(orc_draws* d) {
+    return d->counter ? orc_counter_draw(d->ss, 1024 + d->t++) : orc_rng_next(&d->rng);
+}
+static inline uint64_t orc_draw_jitter(orc_draws* d, int p, int q) {
+    return d->counter ? orc_counter_draw(d->ss, 2048 + 64 * p + q) : orc_rng_next(&d->rng);
 }
 
 /* exported for the RNG known-answer tests */
@@ -142,12 +157,14 @@ typedef struct {
     int64_t n_negs;
 } orc_record;
 
-/* One epoch, serial semantics of epoch_worker<DIM,false> with tid 0 (or a stream per edge when
+/* One epoch, serial semantics of epoch_worker<DIM,false> with tid 0 (or the counter draws when
  * per_edge_stream). apply == 0: only the draws and the eons/eonns bookkeeping (schedule replay). */
 static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float alpha, float mid_w,
                       int per_edge_stream, int apply, orc_record* rec) {
     const int dim = c->dim;
-    orc_rng rng; orc_rng_seed(&rng, orc_stream_seed(c->seed, epoch, 0));
+    orc_draws dr; memset(&dr, 0, sizeof(dr));
+    orc_rng_seed(&dr.rng, orc_stream_seed(c->seed, epoch, 0));
+    dr.counter = per_edge_stream;
     const float fepoch = (float)epoch;
     float* Y = c->Y;
     float diff[ORC_MAX_DIM], gu[ORC_MAX_DIM], gk[ORC_MAX_DIM];
@@ -155,8 +172,7 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
     for (int64_t i = 0; i < c->n_edges; ++i) {
         if (rec) { rec->sampled[i] = 0; rec->n_neg[i] = 0; rec->mid[i] = -1; rec->neg_off[i] = rec->n_negs; }
         if (c->eons[i] > fepoch) continue;
-        const uint64_t sseed = orc_stream_seed(c->seed, epoch, (uint64_t)i);
-        if (per_edge_stream) orc_rng_seed(&rng, sseed);
+        dr.ss = orc_stream_seed(c->seed, epoch, (uint64_t)i); dr.p = 0; dr.t = 0;
         if (rec) rec->sampled[i] = 1;
         const int32_t u = c->head[i], v = c->tail[i];
         float* yu = Y + (int64_t)u * dim;
@@ -184,7 +200,7 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
             const int n_neg = (int)((fepoch - c->eonns[i]) / epn);
             if (rec) rec->n_neg[i] = n_neg > 0 ? n_neg : 0;
             for (int p = 0; p < n_neg; ++p) {
-                const int32_t k = (int32_t)orc_rng_below(&rng, (uint32_t)c->n);
+                const int32_t k = (int32_t)orc_below_of(orc_draw_neg(&dr), (uint32_t)c->n);
                 if (rec && rec->n_negs < rec->negs_cap) rec->negs[rec->n_negs] = k;
                 if (rec) rec->n_negs++;
                 if (k == u) continue;
@@ -207,11 +223,8 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
                         coeff = c->repulsion_strength * 2.0f * c->a * (1.0f - th * th) / th;
                     }
                     for (int q = 0; q < dim; ++q) gu[q] += coeff * diff[q];
-                } else if (per_edge_stream) {
-                    orc_rng jr; orc_jitter_seed(&jr, sseed, p);
-                    for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&jr) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
                 } else {
-                    for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&rng) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+                    for (int q = 0; q < dim; ++q) gu[q] += (orc_uniform_of(orc_draw_jitter(&dr, p, q)) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
                 }
             }
             c->eonns[i] += (float)n_neg * epn;
@@ -220,7 +233,7 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
             const float q_v = 1.0f / (1.0f + c->a * pw_v);
             float Z = q_v;
             for (int p = 0; p < dv->m_neg; ++p) {
-                int32_t k = (int32_t)orc_rng_below(&rng, (uint32_t)c->n);
+                int32_t k = (int32_t)orc_below_of(orc_draw_neg(&dr), (uint32_t)c->n);
                 if (k == u) k = (int32_t)((k + 1) % c->n);
                 negs[p] = k;
                 if (rec && rec->n_negs < rec->negs_cap) rec->negs[rec->n_negs] = k;
@@ -245,12 +258,7 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
                 float dd = 0.0f;
                 for (int q = 0; q < dim; ++q) { diff[q] = yu[q] - yk[q]; dd += diff[q] * diff[q]; }
                 if (dd <= 0.0f) {
-                    if (per_edge_stream) {
-                        orc_rng jr; orc_jitter_seed(&jr, sseed, p);
-                        for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&jr) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
-                    } else {
-                        for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&rng) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
-                    }
+                    for (int q = 0; q < dim; ++q) gu[q] += (orc_uniform_of(orc_draw_jitter(&dr, p, q)) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
                     continue;
                 }
                 const float pw = dv->b_is_one ? dd : powf(dd, c->b);
@@ -263,28 +271,28 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
             c->eonns[i] = fepoch;
         }
         /* mid-range partner (src/layout.cpp:225-255) */
-        if (mid_w > 0.0f && orc_rng_uniform(&rng) < c->mid_rate) {
+        if (mid_w > 0.0f && orc_uniform_of(orc_draw_mid(&dr)) < c->mid_rate) {
             int32_t w = v;
             if (c->jump_indptr && c->mid_jump > 0.0f) {
                 const int L = c->walk_lens ? c->walk_lens[v] : c->walk_len;
                 for (int h = 0; h < L; ++h) {
                     const int32_t js = c->jump_indptr[w], je = c->jump_indptr[w + 1];
-                    if (je > js && orc_rng_uniform(&rng) < c->mid_jump) {
-                        w = c->jump_indices[js + (int32_t)orc_rng_below(&rng, (uint32_t)(je - js))];
+                    if (je > js && orc_uniform_of(orc_draw_mid(&dr)) < c->mid_jump) {
+                        w = c->jump_indices[js + (int32_t)orc_below_of(orc_draw_mid(&dr), (uint32_t)(je - js))];
                     } else {
                         const int32_t s0 = c->indptr[w], e0 = c->indptr[w + 1];
                         if (e0 <= s0) break;
-                        w = c->indices[s0 + (int32_t)orc_rng_below(&rng, (uint32_t)(e0 - s0))];
+                        w = c->indices[s0 + (int32_t)orc_below_of(orc_draw_mid(&dr), (uint32_t)(e0 - s0))];
                     }
                 }
             } else if (c->mid_pairs) {
-                w = c->mid_pairs[(int64_t)u * c->n_mid + orc_rng_below(&rng, (uint32_t)c->n_mid)];
+                w = c->mid_pairs[(int64_t)u * c->n_mid + orc_below_of(orc_draw_mid(&dr), (uint32_t)c->n_mid)];
             } else {
                 const int L = c->walk_lens ? c->walk_lens[v] : c->walk_len;
                 for (int h = 0; h < L; ++h) {
                     const int32_t s0 = c->indptr[w], e0 = c->indptr[w + 1];
                     if (e0 <= s0) break;
-                    w = c->indices[s0 + (int32_t)orc_rng_below(&rng, (uint32_t)(e0 - s0))];
+                    w = c->indices[s0 + (int32_t)orc_below_of(orc_draw_mid(&dr), (uint32_t)(e0 - s0))];
                 }
             }
             if (rec) rec->mid[i] = (w != u) ? w : -2;
@@ -306,8 +314,8 @@ static void orc_sched(const orc_sgd_args* c, const orc_derived* dv, int epoch, f
 }
 
 /* optimize_layout with n_threads = 1, parallel = 0 (hogwild path run on one thread): Y, eons, eonns and the
- * Adam state are updated in place. per_edge_stream = 1 runs the same updates with the GPU fast mode's stream
- * per edge. Returns 0. */
+ * Adam state are updated in place. per_edge_stream = 1 runs the same updates with the GPU fast mode's
+ * counter draws. Returns 0. */
 int orc_sgd_serial(orc_sgd_args* c, int per_edge_stream) {
     orc_derived dv; orc_derive(c, &dv);
     for (int e = c->epoch_start; e < c->epoch_end; ++e) {

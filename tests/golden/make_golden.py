@@ -72,6 +72,16 @@ def sgd_fixture():
         out[f"Y_{name}"] = Y
         out[f"eons_{name}"] = eons
         out[f"eonns_{name}"] = eonns
+        # the same run over 8 more seeds: the spread of the reference's own layout quality
+        seeds = []
+        for sd in range(1, 9):
+            Y = Y0.copy(); eons = eps.copy(); eonns = (eps / 5).astype(np.float32)
+            _magnet.optimize_layout(Y, head, tail, eps, eons, eonns, ip, ix, 0, n_epochs, 1.0, 0.0, mw, 0.0,
+                                    1.7, cfg["b"], 1.7382, 1.0, 5.0, 0, 1.0, 2.0, 4, 0.25, 0, 0, 0,
+                                    np.zeros((0, 2), np.float32), np.zeros((0, 2), np.float32), z, 0.9, 0.999, z, mp,
+                                    z, z, 0.0, 0, np.zeros(0, np.float32), sd, 1, 0)
+            seeds.append(Y)
+        out[f"Yseeds_{name}"] = np.stack(seeds)
     np.savez_compressed(os.path.join(HERE, "sgd_small.npz"), **out)
 
 

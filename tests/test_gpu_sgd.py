@@ -67,8 +67,12 @@ def test_layout_against_reference(mg, golden, stream_mode, case):
     Y, eons, eonns = run_layout(mg, g, stream_mode, case)
     assert np.array_equal(eons, g[f"eons_{case}"]) and np.array_equal(eonns, g[f"eonns_{case}"])
     assert np.isfinite(Y).all()
-    p, p_ref = purity(Y, g["labels"]), purity(g[f"Y_{case}"], g["labels"])
-    assert p > p_ref - 0.03
+    # layout quality over 8 seeds against the reference's own 8 runs (same inputs, seeds 1..8): single runs of
+    # a 600-point layout spread by a few points of purity, so the means are compared (tolerance 0.03)
+    labels = g["labels"]
+    p_ref = np.mean([purity(Yr, labels) for Yr in g[f"Yseeds_{case}"]])
+    p = np.mean([purity(run_layout(mg, g, stream_mode, case, seed=s)[0], labels) for s in range(1, 9)])
+    assert p > p_ref - 0.03, (p, p_ref)
 
 
 def test_serial_stream_mode_is_deterministic(mg, golden):
