@@ -59,6 +59,24 @@ int mg_fftconv_compute(mg_fftconv* h, const float* Y, int64_t n, float xmin, flo
                        int n_boxes, float* sumQ, float* F);
 void mg_fftconv_destroy(mg_fftconv* h);
 
+/* No counterpart in the reference: FFTConv2D(M, n_interp).set_kernels(K1h, K2h).compute(Y, ...) in one call
+ * that allocates nothing, for callers that must not allocate device memory, e.g. a process whose device memory
+ * is already reserved up to its budget, or a thread that must not stall the other streams on the implicit
+ * device synchronisation of cudaMalloc / cudaFree. Same arguments and results as mg_fftconv_create +
+ * mg_fftconv_set_kernels + mg_fftconv_compute, with three limits:
+ *   - M <= mg_fftconv_noalloc_max_side() (512, so n_boxes * n_interp <= 512); larger M returns MG_ERR_ARGUMENT.
+ *   - K1h, K2h ((M, M/2+1) real each), Y, F ((n, 2)) and sumQ must be device memory; nothing is staged.
+ *   - The scratch is one static device array (16.8 MB) per device, shared by all callers of this entry point:
+ *     calls whose work overlaps on the device (two streams, or two host threads) race on it and must be
+ *     serialised by the caller.
+ * The first call on each device looks up the scratch's device address (cudaGetSymbolAddress, which may load
+ * the library's module); make that first call before any stream capture. Asynchronous on the thread's stream
+ * (mg_set_stream). */
+int mg_fftconv_compute_noalloc(const float* K1h, const float* K2h, int M, int n_interp, const float* Y, int64_t n,
+                               float xmin, float ymin, float width, int n_boxes, float* sumQ, float* F);
+/* The largest FFT side M that mg_fftconv_compute_noalloc accepts. */
+int mg_fftconv_noalloc_max_side(void);
+
 /* ================================================================ t-SNE per-iteration kernels (src/fftrep.cpp) */
 /* tsne_attraction (src/fftrep.cpp:129-177): out_i = sum_j p_ij (1 + |y_i - y_j|^2/dof)^-1 (y_i - y_j) over the
  * CSR rows (indptr n+1, indices / data nnz); Y and out (n, dim), 1 <= dim <= 64. */

@@ -222,6 +222,14 @@ extern "C" int mg_fftconv_compute(mg_fftconv* h, const float* Y, int64_t n, floa
 
 extern "C" void mg_fftconv_destroy(mg_fftconv* h) { delete h; }
 
+extern "C" int mg_fftconv_compute_noalloc(const float* K1h, const float* K2h, int M, int n_interp, const float* Y,
+                                          int64_t n, float xmin, float ymin, float width, int n_boxes, float* sumQ,
+                                          float* F) {
+    return guard([&] { fftconv_compute_noalloc(K1h, K2h, M, n_interp, Y, n, xmin, ymin, width, n_boxes, sumQ, F); });
+}
+
+extern "C" int mg_fftconv_noalloc_max_side(void) { return noalloc_max_fft_side(); }
+
 // ============================================================================================== t-SNE kernels
 extern "C" int mg_tsne_attraction(const int32_t* indptr, const int32_t* indices, const float* data, int64_t nnz,
                                   const float* Y, int64_t n, int dim, float dof, float* out) {

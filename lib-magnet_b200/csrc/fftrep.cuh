@@ -56,6 +56,11 @@ void rep_set_spectra_from_host_layout(RepBuffers& b, const float* K1h_dev, const
                                       cudaStream_t s);
 void rep_twiddles(GridDesc* g, RepBuffers& b, cudaStream_t s, bool force);   // recompute tw if g->tw_dirty
 
+// allocation-free FFTConv2D.compute on a static scratch (noalloc.cu); device arrays only
+int noalloc_max_fft_side();
+void fftconv_compute_noalloc(const float* K1h, const float* K2h, int M, int n_interp, const float* Y, int64_t n,
+                             float xmin, float ymin, float width, int n_boxes, float* sumQ, float* F);
+
 // register-tiled engine (fftrep2.cu)
 bool fft2_fits(int Mmax);
 void fft2_build_plans(DevBuf& table, int Mmax);
