@@ -8,6 +8,7 @@
 // spectrum and inverse transform for each output channel, and accumulates Z = sum_k K1h |W0h|^2 / M^2 (the
 // same sum as the reference's sum over points of the interpolated potential 0, by Parseval).
 #include "fftrep.cuh"
+#include "fft3.cuh"
 #include "fft.cuh"
 #include "interp.cuh"
 #include <vector>
@@ -19,6 +20,16 @@ int next_5smooth(int target) {
     if (target <= 1) return 1;
     for (int x = target;; ++x)
         if (fft::is_5smooth(x)) return x;
+}
+
+// Any M >= 2N - 1 gives the same circular convolution of the N live nodes (the kernel is sampled at every offset
+// in (-N, N) on the M torus), so the device loop may skip the few 5-smooth lengths the in-place engine has no
+// plan for (5^5 = 3125 and its multiples need five stages) and take the next one.
+int next_fft_len(int target) {
+    for (int x = next_5smooth(target);; x = next_5smooth(x + 1)) {
+        fft3::Plan p;
+        if (x > fft::kMaxLen || fft3::make_plan(x, p)) return x;
+    }
 }
 
 void ensure_fft_attrs();
@@ -42,19 +53,24 @@ void RepBuffers::alloc(int Nmax_, int Mmax_, int ni_) {
     Kt.ensure((size_t)2 * Mhmax * Mmax * sizeof(float));
     tw.ensure((size_t)Mmax * sizeof(float2));
     zpart.ensure((size_t)Mhmax * sizeof(double));
+    // The in-place engine runs when the largest length has a plan: an FFTConv2D object computes at M = Mmax only,
+    // and the device loop takes its lengths from the table below, which then holds planned lengths only.
+    fft3::Plan pmax;
+    use2 = false;
+    use3 = fft3::make_plan(Mmax, pmax);
+    fft3_build_plans(plans3, Mmax, Mp3max);
+    if (use3) col3_blocks(Mp3max);
     std::vector<int> table(2 * (size_t)Nmax + 2);
     int cur = 1;
     for (size_t t = 0; t < table.size(); ++t) {
-        if ((int)t > cur || t == 0) cur = next_5smooth((int)std::max<size_t>(t, 1));
+        if ((int)t > cur || t == 0) {
+            const int target = (int)std::max<size_t>(t, 1);
+            cur = use3 ? next_fft_len(target) : next_5smooth(target);
+        }
         table[t] = cur;
     }
     fft_len_table.ensure(table.size() * sizeof(int));
     MGB_CUDA(cudaMemcpy(fft_len_table.p, table.data(), table.size() * sizeof(int), cudaMemcpyHostToDevice));
-    use2 = fft2_fits(Mmax);
-    if (use2) {
-        fft2_build_plans(plans, Mmax);
-        ensure_fft2_attrs();
-    }
 }
 
 namespace {
@@ -492,10 +508,14 @@ void rep_convolve(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEve
                                                                 b.Npmax, b.Mhmax, b.tw.as<float2>());
     MGB_LAUNCH_CHECK();
     if (ev) MGB_CUDA(cudaEventRecord(ev[0], s));
-    col_kernel<<<fft_blocks(b.Mhmax), kFftThreads, smem, s>>>(g, b.WhT.as<float2>(), b.PhT.as<float2>(), b.Npmax,
-                                                              b.Mhmax, b.Kt.as<float>(), b.Mmax, b.tw.as<float2>(),
-                                                              b.zpart.as<double>(), n);
-    MGB_LAUNCH_CHECK();
+    if (b.use3) {
+        rep_col3(g, b, n, s);
+    } else {
+        col_kernel<<<fft_blocks(b.Mhmax), kFftThreads, smem, s>>>(g, b.WhT.as<float2>(), b.PhT.as<float2>(), b.Npmax,
+                                                                  b.Mhmax, b.Kt.as<float>(), b.Mmax,
+                                                                  b.tw.as<float2>(), b.zpart.as<double>(), n);
+        MGB_LAUNCH_CHECK();
+    }
     if (ev) MGB_CUDA(cudaEventRecord(ev[1], s));
     row_inv_kernel<<<fft_blocks(pairs), kFftThreads, smem, s>>>(g, b.PhT.as<float2>(), b.Npmax, b.Mhmax,
                                                                 b.phi.as<float>(), b.Nmax, b.tw.as<float2>());

@@ -38,11 +38,16 @@ struct RepBuffers {
     DevBuf W, WhT, PhT, phi, Kt, Rt, tw, zpart, fft_len_table, bbox_part, mean_part, plans;
     int max_bbox_blocks = 0;
     bool use2 = false;        // the register-tiled FFT engine (fftrep2.cu) holds this Mmax
+    DevBuf plans3;            // in-place engine (fft3.cuh) plans, indexed by M
+    int Mp3max = 0;           // its largest padded length up to Mmax
+    bool use3 = false;        // the in-place column pass (fftrep3.cu) runs every length these buffers see
     void alloc(int Nmax_, int Mmax_, int ni_);
 };
 
 // host-side next_fast_len(target, real=True) of scipy: smallest 5-smooth integer >= target
 int next_5smooth(int target);
+// smallest 5-smooth length >= target that the in-place engine has a plan for
+int next_fft_len(int target);
 
 // kernel launches (all asynchronous on stream s; sizes read from the device GridDesc g)
 void rep_set_grid_host(GridDesc* g_dev, float xmin, float ymin, float width, int n_boxes, int ni, int M,
@@ -60,6 +65,11 @@ void rep_twiddles(GridDesc* g, RepBuffers& b, cudaStream_t s, bool force);   // 
 int noalloc_max_fft_side();
 void fftconv_compute_noalloc(const float* K1h, const float* K2h, int M, int n_interp, const float* Y, int64_t n,
                              float xmin, float ymin, float width, int n_boxes, float* sumQ, float* F);
+
+// in-place engine (fftrep3.cu)
+void fft3_build_plans(DevBuf& table, int Mmax, int& Mp_max);
+int col3_blocks(int Mp_max);
+void rep_col3(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s);
 
 // register-tiled engine (fftrep2.cu)
 bool fft2_fits(int Mmax);

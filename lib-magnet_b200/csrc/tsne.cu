@@ -516,7 +516,7 @@ void TsneDev::init(const int32_t* ip_h, const int32_t* ix_h, const float* P_h, i
         MGB_CUDA(cudaMemcpyAsync(P.p, P_h, sizeof(float) * nnz, kind, st));
     }
     const int Nmax = s.max_boxes * s.ni;
-    rb.alloc(Nmax, next_5smooth(2 * Nmax), s.ni);
+    rb.alloc(Nmax, next_fft_len(2 * Nmax), s.ni);
     rep_prepare_device_spectra(rb);
     gdesc.ensure(sizeof(GridDesc));
     MGB_CUDA(cudaMemsetAsync(gdesc.p, 0, sizeof(GridDesc), st));
