@@ -13,7 +13,8 @@
 // inverse stage can write global memory directly, which leaves 2 (S - 1) shared-memory round trips per
 // convolution.
 //
-// Bank conflicts: stages before the last read consecutive positions across threads; the last stage reads R_S
+// Twiddles between stages come from one table read per butterfly (powers by products). Bank conflicts: stages
+// before the last read consecutive positions across threads; the last stage reads R_S
 // consecutive positions per thread. When R_S is even the buffer inserts one slot every R_S elements
 // (pad(i) = i + i / R_S), which makes that stride odd.
 #pragma once
@@ -232,6 +233,27 @@ __device__ __forceinline__ void dft_inv(float2* v) {
         default: F<20>(__VA_ARGS__); break;         \
     }
 
+// v[q] *= w^q for q >= 1 (CONJ: conj(w)^q), w = tw[step]: powers by successive products from one table read,
+// re-read from the table every 8 powers so that the rounding of the recurrence stays within a few ulps
+template <int R, bool CONJ>
+__device__ __forceinline__ void twiddle(float2* v, const float2* __restrict__ tw, int step) {
+    float2 w = __ldg(&tw[step]);
+    if (CONJ) w.y = -w.y;
+    float2 wq = w;
+#pragma unroll
+    for (int q = 1; q < R; ++q) {
+        if (q > 1) {
+            if (q % 8 == 0) {
+                wq = __ldg(&tw[step * q]);
+                if (CONJ) wq.y = -wq.y;
+            } else {
+                wq = fft::cmul(wq, w);
+            }
+        }
+        v[q] = fft::cmul(v[q], wq);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------- stages
 // Each stage function is compiled once per radix (not inlined), processes one or two buffers in one loop over
 // nbuf * M / R butterflies, and is shared by every call site: a plan executes a handful of small functions, which
@@ -263,10 +285,7 @@ __device__ __noinline__ void dif_first(const Plan& p, float2* __restrict__ A, fl
             v[r] = n < n_live ? load(t, n) : make_float2(0.f, 0.f);
         }
         dft_fwd<R>(v);
-        if (b) {
-#pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = fft::cmul(v[q], __ldg(&tw[b * q]));
-        }
+        if (b) twiddle<R, false>(v, tw, b);
         const int base = padR ? b + udiv(b, mpad) : b;
 #pragma unroll
         for (int q = 0; q < R; ++q) buf[base + st.ps * q] = v[q];
@@ -289,10 +308,7 @@ __device__ __noinline__ void dif_mid(const Plan& p, int s, float2* __restrict__ 
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = buf[base + st.ps * r];
         dft_fwd<R>(v);
-        if (j) {
-#pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = fft::cmul(v[q], __ldg(&tw[st.tws * j * q]));
-        }
+        if (j) twiddle<R, false>(v, tw, st.tws * j);
 #pragma unroll
         for (int q = 0; q < R; ++q) buf[base + st.ps * q] = v[q];
     }
@@ -313,10 +329,7 @@ __device__ __noinline__ void dit_mid(const Plan& p, int s, float2* __restrict__ 
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = buf[base + st.ps * r];
-        if (j) {
-#pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = fft::cmul(v[q], fft::cconj(__ldg(&tw[st.tws * j * q])));
-        }
+        if (j) twiddle<R, true>(v, tw, st.tws * j);
         dft_inv<R>(v);
 #pragma unroll
         for (int r = 0; r < R; ++r) buf[base + st.ps * r] = v[r];
@@ -338,10 +351,7 @@ __device__ __noinline__ void dit_last(const Plan& p, const float2* __restrict__ 
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = buf[base + st.ps * r];
-        if (b) {
-#pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = fft::cmul(v[q], fft::cconj(__ldg(&tw[b * q])));
-        }
+        if (b) twiddle<R, true>(v, tw, b);
         dft_inv<R>(v);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -370,6 +380,26 @@ __device__ __forceinline__ int base_freq(const Plan& p, int b) {
         if (s < p.S - 1) { f += q[s] * w; w *= p.st[s].R; }
     }
     return f;
+}
+
+// padded position of frequency f after the forward stages: the digits of f (R_1 least significant) read in
+// the opposite order
+__device__ __forceinline__ int pos_of_freq(const Plan& p, int f) {
+    int q[kMaxStages] = {0, 0, 0, 0};
+    int x = f;
+#pragma unroll
+    for (int s = 0; s < kMaxStages; ++s) {
+        if (s < p.S) {
+            const int y = udiv(x, p.mR[s]);
+            q[s] = x - y * p.st[s].R;
+            x = y;
+        }
+    }
+    int pos = q[0];
+#pragma unroll
+    for (int s = 1; s < kMaxStages; ++s)
+        if (s < p.S) pos = pos * p.st[s].R + q[s];
+    return p.padR ? pos + udiv(pos, p.mpad) : pos;
 }
 
 }  // namespace fft3

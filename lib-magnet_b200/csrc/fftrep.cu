@@ -44,7 +44,7 @@ void RepBuffers::alloc(int Nmax_, int Mmax_, int ni_) {
     Nmax = std::max(Nmax, Nmax_);
     Mmax = std::max(Mmax, Mmax_);
     Mhmax = Mmax / 2 + 1;
-    Npmax = Nmax + (Nmax & 1);
+    Npmax = (Nmax + 3) & ~3;   // transposed spectra of 4 rows at once: 32-byte aligned groups
     W.ensure((size_t)Nmax * Nmax * sizeof(float4));
     MGB_CUDA(cudaMemset(W.p, 0, (size_t)Nmax * Nmax * sizeof(float4)));
     WhT.ensure((size_t)3 * Mhmax * Npmax * sizeof(float2));
@@ -59,7 +59,7 @@ void RepBuffers::alloc(int Nmax_, int Mmax_, int ni_) {
     use2 = false;
     use3 = fft3::make_plan(Mmax, pmax);
     fft3_build_plans(plans3, Mmax, Mp3max);
-    if (use3) col3_blocks(Mp3max);
+    if (use3) fft3_prepare(Mp3max);
     std::vector<int> table(2 * (size_t)Nmax + 2);
     int cur = 1;
     for (size_t t = 0; t < table.size(); ++t) {
@@ -502,20 +502,25 @@ void rep_convolve(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEve
         rep_convolve2(g, b, n, s, ev);
         return;
     }
+    if (b.use3) {
+        rep_row_fwd3(g, b, s);
+        if (ev) MGB_CUDA(cudaEventRecord(ev[0], s));
+        rep_col3(g, b, n, s);
+        if (ev) MGB_CUDA(cudaEventRecord(ev[1], s));
+        rep_row_inv3(g, b, s);
+        if (ev) MGB_CUDA(cudaEventRecord(ev[2], s));
+        return;
+    }
     const size_t smem = fft_smem(b.Mmax);
     const int pairs = (b.Nmax + 1) / 2;
     row_fwd_kernel<<<fft_blocks(pairs), kFftThreads, smem, s>>>(g, b.W.as<float4>(), b.Nmax, b.WhT.as<float2>(),
                                                                 b.Npmax, b.Mhmax, b.tw.as<float2>());
     MGB_LAUNCH_CHECK();
     if (ev) MGB_CUDA(cudaEventRecord(ev[0], s));
-    if (b.use3) {
-        rep_col3(g, b, n, s);
-    } else {
-        col_kernel<<<fft_blocks(b.Mhmax), kFftThreads, smem, s>>>(g, b.WhT.as<float2>(), b.PhT.as<float2>(), b.Npmax,
-                                                                  b.Mhmax, b.Kt.as<float>(), b.Mmax,
-                                                                  b.tw.as<float2>(), b.zpart.as<double>(), n);
-        MGB_LAUNCH_CHECK();
-    }
+    col_kernel<<<fft_blocks(b.Mhmax), kFftThreads, smem, s>>>(g, b.WhT.as<float2>(), b.PhT.as<float2>(), b.Npmax,
+                                                              b.Mhmax, b.Kt.as<float>(), b.Mmax, b.tw.as<float2>(),
+                                                              b.zpart.as<double>(), n);
+    MGB_LAUNCH_CHECK();
     if (ev) MGB_CUDA(cudaEventRecord(ev[1], s));
     row_inv_kernel<<<fft_blocks(pairs), kFftThreads, smem, s>>>(g, b.PhT.as<float2>(), b.Npmax, b.Mhmax,
                                                                 b.phi.as<float>(), b.Nmax, b.tw.as<float2>());

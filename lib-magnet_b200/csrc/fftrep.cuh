@@ -69,7 +69,10 @@ void fftconv_compute_noalloc(const float* K1h, const float* K2h, int M, int n_in
 // in-place engine (fftrep3.cu)
 void fft3_build_plans(DevBuf& table, int Mmax, int& Mp_max);
 int col3_blocks(int Mp_max);
+void fft3_prepare(int Mp_max);
 void rep_col3(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s);
+void rep_row_fwd3(GridDesc* g, RepBuffers& b, cudaStream_t s);
+void rep_row_inv3(GridDesc* g, RepBuffers& b, cudaStream_t s);
 
 // register-tiled engine (fftrep2.cu)
 bool fft2_fits(int Mmax);

@@ -206,6 +206,137 @@ __global__ void __launch_bounds__(kColThreads, 2) col3_kernel(GridDesc* __restri
     }
 }
 
+// ---------------------------------------------------------------------------------------------- rows
+// A block owns 4 grid rows g0..g0+3 (src/fftconv.cpp:129-143 forward, :188-198 inverse). Rows are packed two per
+// complex sequence (z = w_g + i w_{g+1}); buffer A holds the pair (g0, g0+1), buffer B the pair (g0+2, g0+3), so
+// the transposed spectra of the 4 rows are read and written as 32 contiguous bytes per frequency.
+constexpr int kRowThreads = 256;
+
+__device__ __forceinline__ float chan(const float4& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// channel c of rows g0..g0+3 of the charge grid (rows at or past N read as zero)
+struct RowLoad {
+    const float4* W;
+    int pitch, g0, N, c;
+    __device__ __forceinline__ float2 operator()(int t, int n) const {
+        const int ga = g0 + 2 * t, gb = ga + 1;
+        const float x = ga < N ? chan(W[(size_t)ga * pitch + n], c) : 0.f;
+        const float y = gb < N ? chan(W[(size_t)gb * pitch + n], c) : 0.f;
+        return make_float2(x, y);
+    }
+};
+
+// potential channel c of rows g0..g0+3: Re to row g0 + 2t, Im to row g0 + 2t + 1, scaled by 1 / M^2
+struct PhiStore {
+    float* phi;
+    size_t plane;
+    int pitch, g0, N, c;
+    float scale;
+    __device__ __forceinline__ void operator()(int t, int n, float2 v) const {
+        const int ga = g0 + 2 * t, gb = ga + 1;
+        float* base = phi + (size_t)c * plane + n;
+        if (ga < N) base[(size_t)ga * pitch] = v.x * scale;
+        if (gb < N) base[(size_t)gb * pitch] = v.y * scale;
+    }
+};
+
+// Forward row transforms of the 3 charge channels, separated into the half spectra of the 4 rows and written
+// transposed (WhT[c][k][g]); the consumed rows of W are zeroed for the next spread.
+__global__ void __launch_bounds__(kRowThreads, 2) row_fwd3_kernel(const GridDesc* __restrict__ gd,
+                                                                  const fft3::Plan* __restrict__ plans,
+                                                                  float4* __restrict__ W, int pitchW,
+                                                                  float2* __restrict__ WhT, int Np, int Mhmax,
+                                                                  const float2* __restrict__ tw) {
+    extern __shared__ float2 sm[];
+    __shared__ fft3::Plan p;
+    const int N = gd->N, M = gd->M, Mh = gd->Mh;
+    if (threadIdx.x == 0) p = plans[M];
+    __syncthreads();
+    float2* A = sm;
+    float2* B = sm + p.Mp;
+    const int S = p.S;
+    const int groups = (N + 3) / 4;
+    for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+        const int g0 = 4 * grp;
+        const int nbuf = g0 + 2 < N ? 2 : 1;
+        for (int c = 0; c < 3; ++c) {
+            MGB_FFT3_RADIX_DISPATCH(p.st[0].R, fft3::dif_first, p, A, B, nbuf, RowLoad{W, pitchW, g0, N, c}, N, tw);
+            __syncthreads();
+            for (int s = 1; s < S; ++s) {
+                MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dif_mid, p, s, A, B, nbuf, tw);
+                __syncthreads();
+            }
+            // rows a, b of a pair from Z_k and Z_{-k}: (Z_k + conj Z_{-k}) / 2 and (Z_k - conj Z_{-k}) / 2i
+            for (int k = threadIdx.x; k < Mh; k += blockDim.x) {
+                const int pk = fft3::pos_of_freq(p, k);
+                const int pm = fft3::pos_of_freq(p, k == 0 ? 0 : M - k);
+                float2* dst = WhT + ((size_t)c * Mhmax + k) * Np + g0;
+                for (int t = 0; t < nbuf; ++t) {
+                    const float2* buf = t ? B : A;
+                    const float2 zk = buf[pk], zm = buf[pm];
+                    reinterpret_cast<float4*>(dst)[t] = make_float4(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y),
+                                                                    0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+                }
+            }
+            __syncthreads();
+        }
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int rows = min(4, N - g0);
+        for (int i = threadIdx.x; i < rows * N; i += blockDim.x) {
+            const int r = i / N, n = i - r * N;
+            W[(size_t)(g0 + r) * pitchW + n] = z4;
+        }
+    }
+}
+
+// Inverse row transforms of the 4 potential channels: each pair rebuilt from the two half spectra (Hermitian
+// extension, DC and Nyquist imaginary parts dropped as a c2r does) straight into the digit-reversed positions
+// the inverse stages start from, transformed, scaled by 1/M^2 (src/fftconv.cpp:176, 188-198).
+__global__ void __launch_bounds__(kRowThreads, 2) row_inv3_kernel(const GridDesc* __restrict__ gd,
+                                                                  const fft3::Plan* __restrict__ plans,
+                                                                  const float2* __restrict__ PhT, int Np, int Mhmax,
+                                                                  float* __restrict__ phi, int pitchP,
+                                                                  const float2* __restrict__ tw) {
+    extern __shared__ float2 sm[];
+    __shared__ fft3::Plan p;
+    const int N = gd->N, M = gd->M, Mh = gd->Mh;
+    if (threadIdx.x == 0) p = plans[M];
+    __syncthreads();
+    float2* A = sm;
+    float2* B = sm + p.Mp;
+    const int S = p.S;
+    const bool even = (M & 1) == 0;
+    const float scale = 1.f / ((float)M * (float)M);
+    const size_t plane = (size_t)pitchP * pitchP;
+    const int groups = (N + 3) / 4;
+    for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+        const int g0 = 4 * grp;
+        const int nbuf = g0 + 2 < N ? 2 : 1;
+        for (int c = 0; c < 4; ++c) {
+            for (int k = threadIdx.x; k < M; k += blockDim.x) {
+                const int kk = k < Mh ? k : M - k;
+                const float4* src = reinterpret_cast<const float4*>(PhT + ((size_t)c * Mhmax + kk) * Np + g0);
+                const int pos = fft3::pos_of_freq(p, k);
+                for (int t = 0; t < nbuf; ++t) {
+                    const float4 v = src[t];
+                    float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
+                    if (kk == 0 || (even && kk == M / 2)) { a.y = 0.f; b.y = 0.f; }
+                    if (k >= Mh) { a.y = -a.y; b.y = -b.y; }
+                    (t ? B : A)[pos] = make_float2(a.x - b.y, a.y + b.x);   // a + i b
+                }
+            }
+            __syncthreads();
+            for (int s = S - 1; s >= 1; --s) {
+                MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dit_mid, p, s, A, B, nbuf, tw);
+                __syncthreads();
+            }
+            MGB_FFT3_RADIX_DISPATCH(p.st[0].R, fft3::dit_last, p, A, B, nbuf,
+                                    PhiStore{phi, plane, pitchP, g0, N, c, scale}, N, tw);
+            __syncthreads();
+        }
+    }
+}
+
 size_t col3_smem(int Mp_max) { return (size_t)2 * Mp_max * sizeof(float2); }
 
 }  // namespace
@@ -241,6 +372,58 @@ int col3_blocks(int Mp_max) {
     cached_mp = Mp_max;
     cached_blocks = std::max(1, per_sm) * kNumSMs;
     return cached_blocks;
+}
+
+// resident blocks of a row kernel (raises its shared-memory limit once per device)
+int row3_blocks(const void* fn, int Mp_max) {
+    const size_t smem = col3_smem(Mp_max);
+    int dev = 0, optin = 0;
+    MGB_CUDA(cudaGetDevice(&dev));
+    MGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes a;
+    MGB_CUDA(cudaFuncGetAttributes(&a, fn));
+    require(smem + a.sharedSizeBytes <= (size_t)optin, "FFT side too large for the row engine");
+    MGB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    MGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kRowThreads, smem));
+    return std::max(1, per_sm) * kNumSMs;
+}
+
+namespace {
+struct RowBlocks {
+    int dev = -1, mp = -1, fwd = 0, inv = 0;
+} g_row_blocks;
+}  // namespace
+
+// launch sizes of the row kernels (and their shared-memory limits) for this device and buffer size; called when
+// the buffers are sized, before any stream capture
+void fft3_prepare(int Mp_max) {
+    int dev = 0;
+    MGB_CUDA(cudaGetDevice(&dev));
+    col3_blocks(Mp_max);
+    if (g_row_blocks.dev == dev && g_row_blocks.mp == Mp_max) return;
+    g_row_blocks.fwd = row3_blocks((const void*)row_fwd3_kernel, Mp_max);
+    g_row_blocks.inv = row3_blocks((const void*)row_inv3_kernel, Mp_max);
+    g_row_blocks.dev = dev;
+    g_row_blocks.mp = Mp_max;
+}
+
+void rep_row_fwd3(GridDesc* g, RepBuffers& b, cudaStream_t s) {
+    fft3_prepare(b.Mp3max);
+    const int blocks = std::min(g_row_blocks.fwd, (b.Nmax + 3) / 4);
+    row_fwd3_kernel<<<blocks, kRowThreads, col3_smem(b.Mp3max), s>>>(
+        g, b.plans3.as<fft3::Plan>(), b.W.as<float4>(), b.Nmax, b.WhT.as<float2>(), b.Npmax, b.Mhmax,
+        b.tw.as<float2>());
+    MGB_LAUNCH_CHECK();
+}
+
+void rep_row_inv3(GridDesc* g, RepBuffers& b, cudaStream_t s) {
+    fft3_prepare(b.Mp3max);
+    const int blocks = std::min(g_row_blocks.inv, (b.Nmax + 3) / 4);
+    row_inv3_kernel<<<blocks, kRowThreads, col3_smem(b.Mp3max), s>>>(
+        g, b.plans3.as<fft3::Plan>(), b.PhT.as<float2>(), b.Npmax, b.Mhmax, b.phi.as<float>(), b.Nmax,
+        b.tw.as<float2>());
+    MGB_LAUNCH_CHECK();
 }
 
 void rep_col3(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s) {
