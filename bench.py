@@ -300,11 +300,13 @@ def roofline(w, gp, peaks):
     dom = max((k for k in share if k in alg), key=lambda k: share[k])
     ms = sgd_ms if dom == "sgd_epoch" else stages[dom]
     achieved = alg[dom] / (ms * 1e-3) / 1e9
+    traffic = measured_traffic(dom, n)
     fft_pass_bytes = 16.0 * n + 40.0 * N * N + 112.0 * N * Mh + 8.0 * M * Mh
     fft_pass_ms = stages["spread"] + stages["row_fwd"] + stages["col_conv"] + stages["row_inv"]
     return {
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peaks,
-                     "unit": "GB/s", "frac": round(achieved / peaks, 4), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / peaks, 4),
+                     "traffic": None if traffic is None else round(traffic, 0),
                      "alg_bytes_per_launch": alg[dom], "launch_ms": round(ms, 4),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "stages_ms": {k: round(v, 4) for k, v in stages.items()} | {"sgd_epoch": round(sgd_ms, 4)},
@@ -314,6 +316,22 @@ def roofline(w, gp, peaks):
                      "frac": round(fft_pass_bytes / (fft_pass_ms * 1e-3) / 1e9 / peaks, 4)},
         "grid": {"n_boxes": nb_, "N": N, "M": M},
     }
+
+
+def measured_traffic(stage, n):
+    """DRAM bytes per launch of a stage from the committed ncu summary (profiles/dram_traffic_hybrid_300k.md),
+    scaled to this run's size; None when the stage was not captured"""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_hybrid_300k.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    block = text.split("```traffic", 1)[-1].split("```", 1)[0] if "```traffic" in text else ""
+    for line in block.splitlines():
+        f = line.split()
+        if len(f) == 4 and f[0] == stage and f[2] == "n":
+            return float(f[1]) * n / float(f[3])
+    return None
 
 
 def measured_peak():
