@@ -382,6 +382,13 @@ __device__ __forceinline__ int base_freq(const Plan& p, int b) {
     return f;
 }
 
+// frequency held at (unpadded) position pos after the forward stages
+__device__ __forceinline__ int freq_of_pos(const Plan& p, int pos) {
+    const int RS = p.st[p.S - 1].R;
+    const int b = udiv(pos, p.mR[p.S - 1]);
+    return base_freq(p, b) + (p.M / RS) * (pos - b * RS);
+}
+
 // padded position of frequency f after the forward stages: the digits of f (R_1 least significant) read in
 // the opposite order
 __device__ __forceinline__ int pos_of_freq(const Plan& p, int f) {

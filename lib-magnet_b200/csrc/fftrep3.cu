@@ -4,8 +4,9 @@
 // One block per column k of the row half-spectra (persistent over columns). Two shared-memory buffers hold two
 // transforms at once:
 //   phase 1: channels 1 and 2 (x W, y W), each times K2, into outputs 2 and 3;
-//   phase 2: channel 0 (W) once forward; its spectrum times K1 (output 0, and sum K1 |W0h|^2 for Z) and times K2
-//            (output 1) leave the middle stage in the two buffers.
+//   phase 2: channel 0 (W) once forward; sum K1 |W0h|^2 for Z from its spectrum, and its product with K2 into
+//            output 1. The reference's potential K1 x W0 (output 0) is never formed: Z comes from the spectrum
+//            (Parseval) and the gather reads the potentials 1-3 only.
 // The first forward stage reads the live rows (g < N) of WhT from global memory, the last inverse stage writes
 // the live rows of PhT, so a column costs 2 (S - 1) shared-memory passes per transform and no reordering pass.
 // Output convention as the one-radix engine: PhT = unnormalised inverse (M x the circular convolution).
@@ -56,11 +57,11 @@ __device__ __noinline__ void middle1(const fft3::Plan& p, float2* __restrict__ A
     }
 }
 
-// channel 0: one spectrum (in A), two products (K1 into A, K2 into B); returns this thread's share of
-// sum K1 |X|^2
+// channel 0: the last forward stage, this thread's share of sum K1 |X|^2 (for Z), the product with K2 and the
+// first inverse stage (in place in A); returns the share
 template <int R>
-__device__ __noinline__ double middle2(const fft3::Plan& p, float2* __restrict__ A, float2* __restrict__ B,
-                                       const float* __restrict__ K1, const float* __restrict__ K2) {
+__device__ __noinline__ double middle2(const fft3::Plan& p, float2* __restrict__ A, const float* __restrict__ K1,
+                                       const float* __restrict__ K2) {
     const int pb = p.padR ? R + 1 : R;
     const int nb = p.M / R;
     double zs = 0.0;
@@ -71,23 +72,14 @@ __device__ __noinline__ double middle2(const fft3::Plan& p, float2* __restrict__
         for (int r = 0; r < R; ++r) v[r] = A[base + r];
         fft3::dft_fwd<R>(v);
         const int fb = fft3::base_freq(p, b);
-        // the K1 product waits in A (same positions, this thread only) while the K2 product is inverted, so that
-        // one spectrum at a time is live in registers
         float zt = 0.f;
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-            const float k1 = __ldg(&K1[fb + nb * q]);
-            zt += k1 * (v[q].x * v[q].x + v[q].y * v[q].y);
-            A[base + q] = fft::cscale(v[q], k1);
+            const int f = fb + nb * q;
+            zt += __ldg(&K1[f]) * (v[q].x * v[q].x + v[q].y * v[q].y);
+            v[q] = fft::cscale(v[q], __ldg(&K2[f]));
         }
         zs += (double)zt;
-#pragma unroll
-        for (int q = 0; q < R; ++q) v[q] = fft::cscale(v[q], __ldg(&K2[fb + nb * q]));
-        fft3::dft_inv<R>(v);
-#pragma unroll
-        for (int r = 0; r < R; ++r) B[base + r] = v[r];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = A[base + r];
         fft3::dft_inv<R>(v);
 #pragma unroll
         for (int r = 0; r < R; ++r) A[base + r] = v[r];
@@ -95,22 +87,22 @@ __device__ __noinline__ double middle2(const fft3::Plan& p, float2* __restrict__
     return zs;
 }
 
-__device__ __forceinline__ double middle2_dispatch(int R, const fft3::Plan& p, float2* A, float2* B, const float* K1,
+__device__ __forceinline__ double middle2_dispatch(int R, const fft3::Plan& p, float2* A, const float* K1,
                                                    const float* K2) {
     switch (R) {
-        case 2: return middle2<2>(p, A, B, K1, K2);
-        case 3: return middle2<3>(p, A, B, K1, K2);
-        case 4: return middle2<4>(p, A, B, K1, K2);
-        case 5: return middle2<5>(p, A, B, K1, K2);
-        case 6: return middle2<6>(p, A, B, K1, K2);
-        case 8: return middle2<8>(p, A, B, K1, K2);
-        case 9: return middle2<9>(p, A, B, K1, K2);
-        case 10: return middle2<10>(p, A, B, K1, K2);
-        case 12: return middle2<12>(p, A, B, K1, K2);
-        case 15: return middle2<15>(p, A, B, K1, K2);
-        case 16: return middle2<16>(p, A, B, K1, K2);
-        case 18: return middle2<18>(p, A, B, K1, K2);
-        default: return middle2<20>(p, A, B, K1, K2);
+        case 2: return middle2<2>(p, A, K1, K2);
+        case 3: return middle2<3>(p, A, K1, K2);
+        case 4: return middle2<4>(p, A, K1, K2);
+        case 5: return middle2<5>(p, A, K1, K2);
+        case 6: return middle2<6>(p, A, K1, K2);
+        case 8: return middle2<8>(p, A, K1, K2);
+        case 9: return middle2<9>(p, A, K1, K2);
+        case 10: return middle2<10>(p, A, K1, K2);
+        case 12: return middle2<12>(p, A, K1, K2);
+        case 15: return middle2<15>(p, A, K1, K2);
+        case 16: return middle2<16>(p, A, K1, K2);
+        case 18: return middle2<18>(p, A, K1, K2);
+        default: return middle2<20>(p, A, K1, K2);
     }
 }
 
@@ -156,14 +148,15 @@ __global__ void __launch_bounds__(kColThreads, 2) col3_kernel(GridDesc* __restri
         }
         MGB_FFT3_RADIX_DISPATCH(R0, fft3::dit_last, p, A, B, 2, ColStore{dst[2], dst[3]}, N, tw);
         __syncthreads();
-        // ---- phase 2: channel 0, times K1 (and Z) into output 0, times K2 into output 1
+        // ---- phase 2: channel 0: Z (sum K1 |W0h|^2) and times K2 into output 1 (the potential K1 x W0 is not
+        // needed: Z comes from the spectrum, and the gather reads the potentials 1-3 only)
         MGB_FFT3_RADIX_DISPATCH(R0, fft3::dif_first, p, A, B, 1, ColLoad{src[0], src[0]}, N, tw);
         __syncthreads();
         for (int s = 1; s < S - 1; ++s) {
             MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dif_mid, p, s, A, B, 1, tw);
             __syncthreads();
         }
-        double zs = middle2_dispatch(RS, p, A, B, K1, K2);
+        double zs = middle2_dispatch(RS, p, A, K1, K2);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) zs += __shfl_xor_sync(0xffffffffu, zs, o);
         if (lane == 0) red[warp] = zs;
@@ -175,10 +168,10 @@ __global__ void __launch_bounds__(kColThreads, 2) col3_kernel(GridDesc* __restri
             zpart[k] = single ? t : 2.0 * t;
         }
         for (int s = S - 2; s >= 1; --s) {
-            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dit_mid, p, s, A, B, 2, tw);
+            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dit_mid, p, s, A, B, 1, tw);
             __syncthreads();
         }
-        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dit_last, p, A, B, 2, ColStore{dst[0], dst[1]}, N, tw);
+        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dit_last, p, A, B, 1, ColStore{dst[1], dst[1]}, N, tw);
         __syncthreads();
     }
     // last block: Z = sum of the partials / M^2 - n
@@ -266,9 +259,12 @@ __global__ void __launch_bounds__(kRowThreads, 2) row_fwd3_kernel(const GridDesc
                 MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dif_mid, p, s, A, B, nbuf, tw);
                 __syncthreads();
             }
-            // rows a, b of a pair from Z_k and Z_{-k}: (Z_k + conj Z_{-k}) / 2 and (Z_k - conj Z_{-k}) / 2i
-            for (int k = threadIdx.x; k < Mh; k += blockDim.x) {
-                const int pk = fft3::pos_of_freq(p, k);
+            // rows a, b of a pair from Z_k and Z_{-k}: (Z_k + conj Z_{-k}) / 2 and (Z_k - conj Z_{-k}) / 2i; walked in
+            // position order (consecutive threads read consecutive positions), frequencies past M/2 skipped
+            for (int pos = threadIdx.x; pos < M; pos += blockDim.x) {
+                const int k = fft3::freq_of_pos(p, pos);
+                if (k >= Mh) continue;
+                const int pk = p.padR ? pos + fft3::udiv(pos, p.mpad) : pos;
                 const int pm = fft3::pos_of_freq(p, k == 0 ? 0 : M - k);
                 float2* dst = WhT + ((size_t)c * Mhmax + k) * Np + g0;
                 for (int t = 0; t < nbuf; ++t) {
@@ -289,7 +285,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) row_fwd3_kernel(const GridDesc
     }
 }
 
-// Inverse row transforms of the 4 potential channels: each pair rebuilt from the two half spectra (Hermitian
+// Inverse row transforms of the potential channels 1-3: each pair rebuilt from the two half spectra (Hermitian
 // extension, DC and Nyquist imaginary parts dropped as a c2r does) straight into the digit-reversed positions
 // the inverse stages start from, transformed, scaled by 1/M^2 (src/fftconv.cpp:176, 188-198).
 __global__ void __launch_bounds__(kRowThreads, 2) row_inv3_kernel(const GridDesc* __restrict__ gd,
@@ -312,11 +308,15 @@ __global__ void __launch_bounds__(kRowThreads, 2) row_inv3_kernel(const GridDesc
     for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {
         const int g0 = 4 * grp;
         const int nbuf = g0 + 2 < N ? 2 : 1;
-        for (int c = 0; c < 4; ++c) {
-            for (int k = threadIdx.x; k < M; k += blockDim.x) {
+        for (int c = 1; c < 4; ++c) {   // potentials 1-3 (the gather's); plane 0 is not formed
+            // the spectrum enters in position order: consecutive threads write consecutive positions; the loads of
+            // the transposed spectra are one 32-byte sector per frequency in either order
+#pragma unroll 2
+            for (int up = threadIdx.x; up < M; up += blockDim.x) {
+                const int k = fft3::freq_of_pos(p, up);
                 const int kk = k < Mh ? k : M - k;
                 const float4* src = reinterpret_cast<const float4*>(PhT + ((size_t)c * Mhmax + kk) * Np + g0);
-                const int pos = fft3::pos_of_freq(p, k);
+                const int pos = p.padR ? up + fft3::udiv(up, p.mpad) : up;
                 for (int t = 0; t < nbuf; ++t) {
                     const float4 v = src[t];
                     float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);

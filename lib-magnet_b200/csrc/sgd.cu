@@ -3,11 +3,12 @@
 //
 // Two stream modes:
 //  * counter-based (stream_mode 0, default): every draw of a sample is addressed by (seed, epoch, edge, index).
-//    Draw j of edge i in epoch e is the first xorshift64* output of the generator seeded as the reference seeds
-//    its streams (src/layout.cpp:123, splitmix64 then xorshift64*) from stream_seed(seed, e, i) ^ (j * golden
-//    ratio). Negative p is draw p; the mid-range draws are draws 1024, 1025, ...; the distance-0 jitter of
-//    negative p in dimension d is draw 2048 + 64 p + d. Any lane can take any draw directly, so the draws of a
-//    sample need no coordination. With the edges sorted by head (the reference's schedule is the COO of a
+//    The sample of edge i in epoch e has a 32-bit key, the hash of the reference's stream seed
+//    (src/layout.cpp:123) stream_seed(seed, e, i); its draw j is hash32(key + j * 0x9E3779B9) in the high 32
+//    bits of a 64-bit draw, so below(n) and uniform() read it as they read the reference's 64-bit outputs.
+//    Negative p is draw p; the mid-range draws are draws 1024, 1025, ...; the distance-0 jitter of negative p
+//    in dimension d is draw 2048 + 64 p + d. Any lane can take any draw directly with one 32-bit hash, so the
+//    draws of a sample need no coordination. With the edges sorted by head (the reference's schedule is the COO of a
 //    sorted CSR) a group of 8 lanes owns a head row and applies the head's steps one after another, as the
 //    reference's loop does; the tails and partners move through hogwild float2 atomics.
 //  * serial (stream_mode 1): the reference's single stream per epoch (n_threads = 1) is replayed exactly. The
@@ -40,9 +41,20 @@ int blocks_for(int64_t work, int per_block, int cap_per_sm = 16) {
 // ---------------------------------------------------------------------------------------------- draws
 __device__ __forceinline__ uint32_t below_of(uint64_t x, uint32_t n) { return (uint32_t)(((x >> 32) * (uint64_t)n) >> 32); }
 __device__ __forceinline__ float uniform_of(uint64_t x) { return (float)(x >> 40) * (1.0f / 16777216.0f); }
-__device__ __forceinline__ uint64_t counter_draw(uint64_t ss, int j) {
-    Rng r(ss ^ ((uint64_t)j * 0x9E3779B97F4A7C15ULL));
-    return r.next();
+// 32-bit integer hash: "lowbias32" of C. Wellons' hash-prospector (xorshift-multiply rounds, full avalanche)
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+// key of a sample from its 64-bit stream seed
+__device__ __forceinline__ uint32_t sample_key(uint64_t ss) {
+    return hash32((uint32_t)ss ^ hash32((uint32_t)(ss >> 32)));
+}
+// draw j of a sample, in the high half of a 64-bit draw
+__device__ __forceinline__ uint64_t counter_draw(uint32_t key, int j) {
+    return (uint64_t)hash32(key + (uint32_t)j * 0x9E3779B9u) << 32;
 }
 
 // the reference's order: one stream, consumed in sequence
@@ -54,12 +66,12 @@ struct SerialDraws {
 };
 // the counter-based draws of the fast mode
 struct CounterDraws {
-    uint64_t ss;
+    uint32_t key;
     int p = 0, t = 0;
-    __device__ __forceinline__ explicit CounterDraws(uint64_t s) : ss(s) {}
-    __device__ __forceinline__ uint64_t neg() { return counter_draw(ss, p++); }
-    __device__ __forceinline__ uint64_t mid() { return counter_draw(ss, kMidDraw + t++); }
-    __device__ __forceinline__ uint64_t jitter(int pi, int d) { return counter_draw(ss, kJitterDraw + 64 * pi + d); }
+    __device__ __forceinline__ explicit CounterDraws(uint32_t k) : key(k) {}
+    __device__ __forceinline__ uint64_t neg() { return counter_draw(key, p++); }
+    __device__ __forceinline__ uint64_t mid() { return counter_draw(key, kMidDraw + t++); }
+    __device__ __forceinline__ uint64_t jitter(int pi, int d) { return counter_draw(key, kJitterDraw + 64 * pi + d); }
 };
 
 // ---------------------------------------------------------------------------------------------- steps
@@ -360,7 +372,7 @@ __global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const
     const int64_t n_groups = (int64_t)gridDim.x * (blockDim.x / kGroup);
     const int role = gl < kNegPerRound ? 0 : (gl == kNegPerRound ? 1 : 2);   // negative / attraction / mid-range
     const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
-    // the common coefficient path: kernel 0 without per-node b, one powf per lane
+    // the common coefficient path: kernel 0 without per-node b, the same instructions on every lane
     const bool uniform_path = c.kernel == 0 && !c.node_b;
     const float ex = role == 1 ? c.b : c.rep_b;
     const bool plain = role == 1 ? c.b_is_one : c.rep_b_is_one;
@@ -400,7 +412,7 @@ __global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const
             have = true;
         }
         const int32_t v = c.tail[i];
-        const uint64_t ss = stream_seed(c.seed, epoch, (uint64_t)i);
+        const uint32_t key = sample_key(stream_seed(c.seed, epoch, (uint64_t)i));
         float gu[D];
 #pragma unroll
         for (int d = 0; d < D; ++d) gu[d] = 0.0f;
@@ -411,14 +423,14 @@ __global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const
             int32_t partner = -1;
             if (role == 0) {
                 if (p < n_neg) {
-                    const int32_t k = (int32_t)below_of(counter_draw(ss, p), (uint32_t)c.n);
+                    const int32_t k = (int32_t)below_of(counter_draw(key, p), (uint32_t)c.n);
                     partner = k == (int32_t)u ? -1 : k;
                 }
             } else if (r == 0) {
                 if (role == 1) {
                     partner = v;
                 } else if (mid_w > 0.0f) {
-                    CounterDraws dr(ss);
+                    CounterDraws dr(key);
                     if (uniform_of(dr.mid()) < c.mid_rate) {
                         const int32_t w = mid_partner(c, (int32_t)u, v, dr);
                         partner = w == (int32_t)u ? -1 : w;
@@ -435,9 +447,12 @@ __global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const
                 const bool pos = d2 > 0.0f;
                 float coeff;
                 if (uniform_path) {
-                    const float pw = (plain || !pos) ? d2 : powf(d2, ex);
-                    const float att = -c.exaggeration * 2.0f * c.a * c.b * pw / (d2 * (c.a * pw + 1.0f));
-                    const float rep = c.two_b / ((0.001f + d2) * (c.rep_a * pw + 1.0f));
+                    // every lane evaluates the same few instructions: d2^ex through log2 / exp2 and fast
+                    // divisions (a few ulp; d2 = 0 gives pw = 0, its coefficient is masked below)
+                    const float pw_e = exp2f(ex * __log2f(d2));
+                    const float pw = plain ? d2 : pw_e;
+                    const float att = __fdividef(-c.exaggeration * 2.0f * c.a * c.b * pw, d2 * (c.a * pw + 1.0f));
+                    const float rep = __fdividef(c.two_b, (0.001f + d2) * (c.rep_a * pw + 1.0f));
                     coeff = role == 0 ? rep : (role == 1 ? att : -mid_w);
                 } else if (role == 0) {
                     coeff = pos ? repulsion_coeff(c, d2, (int32_t)u) : 0.0f;
@@ -455,7 +470,7 @@ __global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const
                 if (role == 0 && !pos) {
 #pragma unroll
                     for (int d = 0; d < D; ++d)
-                        gu[d] += (uniform_of(counter_draw(ss, kJitterDraw + 64 * p + d)) - 0.5f) * jit;
+                        gu[d] += (uniform_of(counter_draw(key, kJitterDraw + 64 * p + d)) - 0.5f) * jit;
                 }
                 const bool moves = ((role == 1 && pos) || role == 2) && partner >= c.n_fixed;
                 if (moves) HogwildSink().template apply<D>(c, partner, gk, alpha, D);
@@ -479,6 +494,217 @@ __global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const
     }
 }
 
+// ---------------------------------------------------------------------------------------------- list kernels
+// The counter mode's fast path (loss 0, dim 2 or 3, edges sorted by head) runs an epoch as two kernels:
+// compact_schedule_kernel writes each row's sampled edges as a compact list, then hogwild_list_kernel gives each
+// row to one thread, which does the row's samples in order, so the head's steps follow one another as in the
+// reference's loop. A sample first gathers what it reads (its list entry, tail, draws, the positions of its tail
+// and negatives), then computes.
+constexpr int kNegBatch = 6;   // n_neg is 4-6 for almost every sample (its long-run mean is the rate, 5)
+
+template <int D>
+__device__ __forceinline__ void load_pos(const float* __restrict__ Y, int64_t k, float* out) {
+    if constexpr (D == 2) {
+        const float2 q = reinterpret_cast<const float2*>(Y)[k];
+        out[0] = q.x; out[1] = q.y;
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) out[d] = Y[k * D + d];
+    }
+}
+
+// what a sample reads before it computes
+template <int D>
+struct Fetched {
+    int64_t i;
+    int nn;
+    int32_t v;
+    uint32_t key;
+    float yv[D];
+    int32_t k[kNegBatch];
+    float yk[kNegBatch][D];
+};
+
+template <int D>
+__device__ __forceinline__ void fetch_sample(const SgdDev& c, int64_t i, int nn, int epoch, Fetched<D>& f) {
+    f.i = i;
+    f.nn = nn;
+    f.v = c.tail[i];
+    f.key = sample_key(stream_seed(c.seed, epoch, (uint64_t)i));
+    load_pos<D>(c.Y, f.v, f.yv);
+#pragma unroll
+    for (int q = 0; q < kNegBatch; ++q) {
+        f.k[q] = q < nn ? (int32_t)below_of(counter_draw(f.key, q), (uint32_t)c.n) : -1;
+        if (f.k[q] >= 0) load_pos<D>(c.Y, f.k[q], f.yk[q]);
+    }
+}
+
+// repulsion of negative k at position yk (dd = |yu - yk|^2): the common path (kernel 0, no per-node b) evaluates
+// d^(2 rep_b) through log2 / exp2 (or directly when rep_b = 1) with a fast division (a few ulp)
+template <int D, bool FAST, bool REP1>
+__device__ __forceinline__ void add_negative(const SgdDev& c, int64_t u, const float* yu, const float* yk,
+                                             uint32_t key, int p, float jit, float* gu) {
+    float diff[D], dd = 0.0f;
+#pragma unroll
+    for (int d = 0; d < D; ++d) { diff[d] = yu[d] - yk[d]; dd = __fadd_rn(dd, __fmul_rn(diff[d], diff[d])); }
+    if (dd > 0.0f) {
+        float coeff;
+        if constexpr (FAST) {
+            const float pw = REP1 ? dd : exp2f(c.rep_b * __log2f(dd));
+            coeff = __fdividef(c.two_b, (0.001f + dd) * (c.rep_a * pw + 1.0f));
+        } else {
+            coeff = repulsion_coeff(c, dd, (int32_t)u);
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) gu[d] += coeff * diff[d];
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) gu[d] += (uniform_of(counter_draw(key, kJitterDraw + 64 * p + d)) - 0.5f) * jit;
+    }
+}
+
+// One sample: the steps of epoch_worker (src/layout.cpp:145-256) in the reference's order (attraction and the
+// tail's step, negatives, mid-range partner, the head's step) with counter draws.
+template <int D, bool FAST, bool REP1, bool B1>
+__device__ __forceinline__ void compute_sample(const SgdDev& c, int64_t u, const Fetched<D>& f, float alpha,
+                                               float mid_w, float jit, float* yu) {
+    float gu[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) gu[d] = 0.0f;
+    {
+        float diff[D], d2 = 0.0f;
+#pragma unroll
+        for (int d = 0; d < D; ++d) { diff[d] = yu[d] - f.yv[d]; d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d])); }
+        if (d2 > 0.0f) {
+            float coeff;
+            if constexpr (FAST) {
+                const float pw = B1 ? d2 : exp2f(c.b * __log2f(d2));
+                coeff = __fdividef(-c.exaggeration * 2.0f * c.a * c.b * pw, d2 * (c.a * pw + 1.0f));
+            } else {
+                const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[f.v]) : c.b;
+                const float pw_v = (c.b_is_one && !c.node_b) ? d2 : powf(d2, b_uv);
+                coeff = attraction_coeff(c, d2, b_uv, pw_v);
+            }
+            float gk[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
+            if (f.v >= c.n_fixed) HogwildSink().template apply<D>(c, f.v, gk, alpha, D);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kNegBatch; ++q)
+        if (f.k[q] >= 0 && f.k[q] != (int32_t)u) add_negative<D, FAST, REP1>(c, u, yu, f.yk[q], f.key, q, jit, gu);
+    for (int p = kNegBatch; p < f.nn; ++p) {   // rare: more negatives than one batch
+        const int32_t k = (int32_t)below_of(counter_draw(f.key, p), (uint32_t)c.n);
+        if (k == (int32_t)u) continue;
+        float yk[D];
+        load_pos<D>(c.Y, k, yk);
+        add_negative<D, FAST, REP1>(c, u, yu, yk, f.key, p, jit, gu);
+    }
+    if (mid_w > 0.0f) {
+        CounterDraws dr(f.key);
+        if (uniform_of(dr.mid()) < c.mid_rate) {
+            const int32_t w = mid_partner(c, (int32_t)u, f.v, dr);
+            if (w != (int32_t)u) {
+                float yw[D], gk[D];
+                load_pos<D>(c.Y, w, yw);
+#pragma unroll
+                for (int d = 0; d < D; ++d) { const float g = -mid_w * (yu[d] - yw[d]); gu[d] += g; gk[d] = -g; }
+                if (w >= c.n_fixed) HogwildSink().template apply<D>(c, w, gk, alpha, D);
+            }
+        }
+    }
+    if (u >= c.n_fixed) local_step<D>(c, yu, gu, alpha, u, D);
+}
+
+// Schedule of an epoch as per-row compact lists. A warp takes a run of whole rows and walks their edges 32 at a
+// time, across row boundaries (coalesced, every lane busy): it runs the schedule of each edge (eons / eonns advance
+// as in the reference) and writes the sampled ones, in order, at the start of their row's own edge range:
+// samp[eptr[u] + j] = edge, nneg[...] = its negatives; rcnt[u] = the row's count. A sampled edge's rank in its row
+// is the count of sampled edges of the same row in lower lanes (the row's lanes form a run, the heads being
+// sorted) plus those of the row in the warp's previous chunks. No global scan is needed, since a row's list fits in its own range.
+__global__ void __launch_bounds__(kThreads) compact_schedule_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+                                                                    int epoch, int64_t rows_per_warp,
+                                                                    int32_t* __restrict__ samp,
+                                                                    int32_t* __restrict__ nneg,
+                                                                    int32_t* __restrict__ rcnt) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lower = (1u << lane) - 1u;
+    const float fepoch = (float)epoch;
+    const int64_t r0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * rows_per_warp;
+    if (r0 >= c.n) return;
+    const int64_t r1 = r0 + rows_per_warp < c.n ? r0 + rows_per_warp : c.n;
+    for (int64_t u = r0 + lane; u < r1; u += 32) rcnt[u] = 0;   // rows without edges keep 0
+    __syncwarp();
+    const int64_t es = eptr[r0], ee = eptr[r1];
+    int32_t carry_row = -1;   // the row that continues from the previous chunk, and its count so far
+    int carry = 0;
+    for (int64_t base = es; base < ee; base += 32) {
+        const int64_t i = base + lane;
+        const bool valid = i < ee;
+        const int32_t h = valid ? c.head[i] : -1;
+        const int nn = valid ? schedule_edge(c, i, fepoch) : -1;
+        const unsigned flags = __ballot_sync(0xffffffffu, nn >= 0);
+        // heads are sorted, so the lanes of a row form a run: [its start lane, the next start lane)
+        const int32_t h_prev = __shfl_up_sync(0xffffffffu, h, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || h != h_prev);
+        const unsigned upto = lane == 31 ? 0xffffffffu : (2u << lane) - 1u;   // lanes <= this one
+        const int run0 = 31 - __clz(starts & upto);
+        const unsigned after = starts & ~upto;
+        const int run1 = after ? __ffs(after) - 1 : 32;
+        const unsigned peers = (unsigned)((1ull << run1) - (1ull << run0));
+        const int before = (h == carry_row) ? carry : 0;
+        if (nn >= 0) {
+            const int64_t slot = eptr[h] + before + __popc(peers & flags & lower);
+            samp[slot] = (int32_t)i;
+            nneg[slot] = nn;
+        }
+        const int total = before + __popc(peers & flags);
+        int32_t nh = -1;   // head of the first edge of the next chunk
+        if (lane == 0 && base + 32 < ee) nh = c.head[base + 32];
+        nh = __shfl_sync(0xffffffffu, nh, 0);
+        const bool last_of_row = lane == 31 - __clz(peers);
+        if (valid && last_of_row && !(lane == 31 && nh == h)) rcnt[h] = total;
+        const int32_t h31 = __shfl_sync(0xffffffffu, h, 31);
+        const int t31 = __shfl_sync(0xffffffffu, total, 31);
+        if (h31 >= 0 && nh == h31) { carry_row = h31; carry = t31; } else { carry_row = -1; carry = 0; }
+    }
+}
+
+template <int D, bool FAST, bool REP1, bool B1>
+__global__ void __launch_bounds__(kThreads, 4) hogwild_list_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+                                                                const int32_t* __restrict__ samp,
+                                                                const int32_t* __restrict__ nneg,
+                                                                const int32_t* __restrict__ rcnt, int epoch,
+                                                                float alpha, float mid_w) {
+    const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < c.n; u += (int64_t)gridDim.x * blockDim.x) {
+        const int cnt = rcnt[u];
+        if (cnt == 0) continue;
+        const int64_t e0 = eptr[u];
+        float yu[D], y0[D];
+        load_pos<D>(c.Y, u, yu);
+#pragma unroll
+        for (int d = 0; d < D; ++d) y0[d] = yu[d];
+        for (int j = 0; j < cnt; ++j) {
+            Fetched<D> f;
+            fetch_sample<D>(c, samp[e0 + j], nneg[e0 + j], epoch, f);
+            compute_sample<D, FAST, REP1, B1>(c, u, f, alpha, mid_w, jit, yu);
+        }
+        if (u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+    }
+}
+
+template <int D, bool FAST>
+void launch_list(const SgdDev& c, int blocks, const int64_t* eptr, const int32_t* samp, const int32_t* nneg,
+                 const int32_t* rcnt, int epoch, float alpha, float mid_w, cudaStream_t s) {
+    const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
+    if (rep1 && b1) hogwild_list_kernel<D, FAST, true, true><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
+    else if (rep1) hogwild_list_kernel<D, FAST, true, false><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
+    else if (b1) hogwild_list_kernel<D, FAST, false, true><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
+    else hogwild_list_kernel<D, FAST, false, false><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
+}
+
 // Row kernel (any dim, any loss): one thread owns a head row and walks it in order with counter draws.
 template <int D>
 __global__ void __launch_bounds__(kThreads) hogwild_rows_kernel(SgdDev c, const int64_t* __restrict__ eptr, int epoch,
@@ -494,7 +720,7 @@ __global__ void __launch_bounds__(kThreads) hogwild_rows_kernel(SgdDev c, const 
             const int n_neg = schedule_edge(c, i, fepoch);
             if (n_neg < 0) continue;
             if (!any) { load_row<D>(c.Y, u, dim, yu); for (int d = 0; d < dim; ++d) y0[d] = yu[d]; any = true; }
-            CounterDraws dr(stream_seed(c.seed, epoch, (uint64_t)i));
+            CounterDraws dr(sample_key(stream_seed(c.seed, epoch, (uint64_t)i)));
             process_edge<D>(c, i, n_neg, alpha, mid_w, dr, HogwildSink(), nullptr, yu, c.Y);
         }
         if (any && u >= c.n_fixed) flush_head<D>(c, u, dim, yu, y0);
@@ -514,7 +740,7 @@ __global__ void __launch_bounds__(kThreads) hogwild_edges_kernel(SgdDev c, int e
         float yu[DM], y0[DM];
         load_row<D>(c.Y, u, dim, yu);
         for (int d = 0; d < dim; ++d) y0[d] = yu[d];
-        CounterDraws dr(stream_seed(c.seed, epoch, (uint64_t)i));
+        CounterDraws dr(sample_key(stream_seed(c.seed, epoch, (uint64_t)i)));
         process_edge<D>(c, i, n_neg, alpha, mid_w, dr, HogwildSink(), nullptr, yu, c.Y);
         if (u >= c.n_fixed) flush_head<D>(c, u, dim, yu, y0);
     }
@@ -649,7 +875,7 @@ __global__ void record_kernel(SgdDev c, int epoch, float alpha, float mid_w, con
         float yu[DM];
         load_row<D>(c.Y, c.head[i], dim, yu);
         if (per_edge) {
-            CounterDraws dr(stream_seed(c.seed, epoch, (uint64_t)i));
+            CounterDraws dr(sample_key(stream_seed(c.seed, epoch, (uint64_t)i)));
             process_edge<D>(c, i, k, alpha, mid_w, dr, NullSink(), &rec, yu, c.Y);
         } else {
             SerialDraws dr{Rng(0)};
@@ -690,12 +916,37 @@ __global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64
     if (threadIdx.x == 0) *total = carry;
 }
 
+// Rows (or edges) in flight at once: at most n / 8 (and at least 64), so that at most about 12 % of the layout
+// moves between a row's read of a position and its own write; small layouts otherwise update every row at once
+// against stale positions. The reference bounds its hogwild threads for the same reason (one per 4096 edges,
+// src/layout.cpp:421). At n = 1M the bound is close to what the device holds resident.
+int64_t max_in_flight(const SgdDev& c) { return std::max<int64_t>(64, c.n / 8); }
+
 template <int D>
-void hogwild_epoch(const SgdDev& c, const int64_t* eptr, int epoch, float alpha, float mid_w, cudaStream_t s) {
-    if (eptr && c.loss == 0 && (D == 2 || D == 3))
-        hogwild_warps_kernel<D == 0 ? 2 : D><<<blocks_for(c.n, kThreads / kGroup, 8), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
-    else if (eptr) hogwild_rows_kernel<D><<<blocks_for(c.n, kThreads), kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
-    else hogwild_edges_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, alpha, mid_w);
+void hogwild_epoch(const SgdDev& c, SgdWork& w, const int64_t* eptr, int epoch, float alpha, float mid_w,
+                   cudaStream_t s) {
+    const int64_t cap = max_in_flight(c);
+    if (eptr && c.loss == 0 && (D == 2 || D == 3)) {
+        int32_t* samp = w.samp.as<int32_t>();
+        int32_t* nneg = w.nneg.as<int32_t>();
+        int32_t* rcnt = w.rcnt.as<int32_t>();
+        const int64_t warps = (int64_t)kNumSMs * 64;   // one resident wave of warps
+        const int64_t rows_per_warp = std::max<int64_t>(1, (c.n + warps - 1) / warps);
+        const int64_t n_warps = (c.n + rows_per_warp - 1) / rows_per_warp;
+        compact_schedule_kernel<<<(int)((n_warps + kThreads / 32 - 1) / (kThreads / 32)), kThreads, 0, s>>>(
+            c, eptr, epoch, rows_per_warp, samp, nneg, rcnt);
+        MGB_LAUNCH_CHECK();
+        const int blocks = (int)std::min<int64_t>(blocks_for(c.n, kThreads, 8), (cap + kThreads - 1) / kThreads);
+        constexpr int DD = D == 0 ? 2 : D;
+        if (c.kernel == 0 && !c.node_b) launch_list<DD, true>(c, blocks, eptr, samp, nneg, rcnt, epoch, alpha, mid_w, s);
+        else launch_list<DD, false>(c, blocks, eptr, samp, nneg, rcnt, epoch, alpha, mid_w, s);
+    } else if (eptr) {
+        const int blocks = (int)std::min<int64_t>(blocks_for(c.n, kThreads), (cap + kThreads - 1) / kThreads);
+        hogwild_rows_kernel<D><<<blocks, kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
+    } else {
+        const int blocks = (int)std::min<int64_t>(blocks_for(c.n_edges, kThreads), (cap + kThreads - 1) / kThreads);
+        hogwild_edges_kernel<D><<<blocks, kThreads, 0, s>>>(c, epoch, alpha, mid_w);
+    }
 }
 
 template <int D>
@@ -761,10 +1012,15 @@ void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha
              float mid_w1, cudaStream_t s) {
     const int64_t* eptr = row_pointers(c, w, s);
     if (stream_mode == 0) {
+        if (eptr && c.loss == 0 && (c.dim == 2 || c.dim == 3)) {
+            w.samp.ensure(sizeof(int32_t) * std::max<int64_t>(c.n_edges, 1));
+            w.nneg.ensure(sizeof(int32_t) * std::max<int64_t>(c.n_edges, 1));
+            w.rcnt.ensure(sizeof(int32_t) * std::max<int64_t>(c.n, 1));
+        }
         for (int e = e0; e < e1; ++e) {
             float alpha, mid_w;
             sgd_sched(c, e, e0, e1, alpha0, alpha1, mid_w0, mid_w1, alpha, mid_w);
-            MGB_DIM_DISPATCH(c.dim, hogwild_epoch, c, eptr, e, alpha, mid_w, s);
+            MGB_DIM_DISPATCH(c.dim, hogwild_epoch, c, w, eptr, e, alpha, mid_w, s);
             MGB_LAUNCH_CHECK();
         }
         return;

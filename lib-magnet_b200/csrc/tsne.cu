@@ -256,23 +256,30 @@ __global__ void __launch_bounds__(kThreads) loop_iter_kernel(const float2* __res
             ax += __shfl_xor_sync(gmask, ax, o, T);
             ay += __shfl_xor_sync(gmask, ay, o, T);
         }
+        // gather of the potentials at the NI x NI stencil (src/fftconv.cpp:211-222), the nodes split over the
+        // row's lanes (node q on lane q mod T) and summed by shuffles
+        int bx, by;
+        float wx[NI], wy[NI];
+        locate<NI>(yi.x, yi.y, xmin, ymin, width, inv_w, nb, bx, by, wx, wy);
+        float p1 = 0.f, p2 = 0.f, p3 = 0.f;
+        for (int q = lg; q < NI * NI; q += T) {
+            const int a = q / NI, b = q - a * NI;
+            float wa = 0.f, wb = 0.f;
+#pragma unroll
+            for (int t = 0; t < NI; ++t) { if (t == a) wa = wx[t]; if (t == b) wb = wy[t]; }
+            const float w = wa * wb;
+            const size_t node = (size_t)(bx * NI + a) * pitchP + (size_t)by * NI + b;
+            p1 += w * __ldg(&phi[plane + node]);
+            p2 += w * __ldg(&phi[2 * plane + node]);
+            p3 += w * __ldg(&phi[3 * plane + node]);
+        }
+#pragma unroll
+        for (int o = T / 2; o > 0; o >>= 1) {
+            p1 += __shfl_xor_sync(gmask, p1, o, T);
+            p2 += __shfl_xor_sync(gmask, p2, o, T);
+            p3 += __shfl_xor_sync(gmask, p3, o, T);
+        }
         if (lg == 0) {
-            // gather in the reference's node order (src/fftconv.cpp:211-222)
-            int bx, by;
-            float wx[NI], wy[NI];
-            locate<NI>(yi.x, yi.y, xmin, ymin, width, inv_w, nb, bx, by, wx, wy);
-            float p1 = 0.f, p2 = 0.f, p3 = 0.f;
-#pragma unroll
-            for (int a = 0; a < NI; ++a) {
-                const size_t row = (size_t)(bx * NI + a) * pitchP + (size_t)by * NI;
-#pragma unroll
-                for (int b = 0; b < NI; ++b) {
-                    const float w = wx[a] * wy[b];
-                    p1 = __fadd_rn(p1, __fmul_rn(w, __ldg(&phi[plane + row + b])));
-                    p2 = __fadd_rn(p2, __fmul_rn(w, __ldg(&phi[2 * plane + row + b])));
-                    p3 = __fadd_rn(p3, __fmul_rn(w, __ldg(&phi[3 * plane + row + b])));
-                }
-            }
             const float fx = __fsub_rn(__fmul_rn(p1, yi.x), p2), fy = __fsub_rn(__fmul_rn(p1, yi.y), p3);
             float2 u = U[i], gn = G[i];
             const float gx_ = __fsub_rn(__fmul_rn(rho, ax), __fmul_rn(fx, inv_sumQ));

@@ -55,25 +55,35 @@ static inline uint64_t orc_stream_seed(uint64_t seed, int epoch, uint64_t tid) {
 }
 
 /* Draw sources of one sample. Serial: the epoch's single stream, consumed in order (the reference).
- * Counter (the device's fast mode): draw j of edge i in epoch e is the first output of the generator seeded with
- * orc_stream_seed(seed, e, i) ^ (j * 0x9E3779B97F4A7C15); negative p is draw p, the mid-range draws are draws
- * 1024, 1025, ..., and the distance-0 jitter of negative p in dimension q is draw 2048 + 64 p + q. */
-typedef struct { orc_rng rng; int counter; uint64_t ss; int p, t; } orc_draws;
+ * Counter (the device's fast mode): the sample of edge i in epoch e has the 32-bit key
+ * orc_hash32(lo ^ orc_hash32(hi)) of its stream seed orc_stream_seed(seed, e, i); its draw j is
+ * orc_hash32(key + j * 0x9E3779B9) in the high 32 bits of a 64-bit draw. Negative p is draw p, the mid-range draws
+ * are draws 1024, 1025, ..., and the distance-0 jitter of negative p in dimension q is draw 2048 + 64 p + q. */
+typedef struct { orc_rng rng; int counter; uint32_t key; int p, t; } orc_draws;
 
-static inline uint64_t orc_counter_draw(uint64_t ss, int j) {
-    orc_rng r; orc_rng_seed(&r, ss ^ ((uint64_t)j * 0x9E3779B97F4A7C15ULL));
-    return orc_rng_next(&r);
+/* 32-bit integer hash "lowbias32" (C. Wellons, hash-prospector): xorshift-multiply rounds */
+static inline uint32_t orc_hash32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+static inline uint32_t orc_sample_key(uint64_t ss) {
+    return orc_hash32((uint32_t)ss ^ orc_hash32((uint32_t)(ss >> 32)));
+}
+static inline uint64_t orc_counter_draw(uint32_t key, int j) {
+    return (uint64_t)orc_hash32(key + (uint32_t)j * 0x9E3779B9u) << 32;
 }
 static inline uint32_t orc_below_of(uint64_t x, uint32_t n) { return (uint32_t)(((x >> 32) * (uint64_t)n) >> 32); }
 static inline float orc_uniform_of(uint64_t x) { return (float)(x >> 40) * (1.0f / 16777216.0f); }
 static inline uint64_t orc_draw_neg(orc_draws* d) {
-    return d->counter ? orc_counter_draw(d->ss, d->p++) : orc_rng_next(&d->rng);
+    return d->counter ? orc_counter_draw(d->key, d->p++) : orc_rng_next(&d->rng);
 }
 static inline uint64_t orc_draw_mid(orc_draws* d) {
-    return d->counter ? orc_counter_draw(d->ss, 1024 + d->t++) : orc_rng_next(&d->rng);
+    return d->counter ? orc_counter_draw(d->key, 1024 + d->t++) : orc_rng_next(&d->rng);
 }
 static inline uint64_t orc_draw_jitter(orc_draws* d, int p, int q) {
-    return d->counter ? orc_counter_draw(d->ss, 2048 + 64 * p + q) : orc_rng_next(&d->rng);
+    return d->counter ? orc_counter_draw(d->key, 2048 + 64 * p + q) : orc_rng_next(&d->rng);
 }
 
 /* exported for the RNG known-answer tests */
@@ -172,7 +182,7 @@ static void orc_epoch(orc_sgd_args* c, const orc_derived* dv, int epoch, float a
     for (int64_t i = 0; i < c->n_edges; ++i) {
         if (rec) { rec->sampled[i] = 0; rec->n_neg[i] = 0; rec->mid[i] = -1; rec->neg_off[i] = rec->n_negs; }
         if (c->eons[i] > fepoch) continue;
-        dr.ss = orc_stream_seed(c->seed, epoch, (uint64_t)i); dr.p = 0; dr.t = 0;
+        dr.key = orc_sample_key(orc_stream_seed(c->seed, epoch, (uint64_t)i)); dr.p = 0; dr.t = 0;
         if (rec) rec->sampled[i] = 1;
         const int32_t u = c->head[i], v = c->tail[i];
         float* yu = Y + (int64_t)u * dim;
