@@ -9,8 +9,8 @@
 //    Negative p is draw p; the mid-range draws are draws 1024, 1025, ...; the distance-0 jitter of negative p
 //    in dimension d is draw 2048 + 64 p + d. Any lane can take any draw directly with one 32-bit hash, so the
 //    draws of a sample need no coordination. With the edges sorted by head (the reference's schedule is the COO of a
-//    sorted CSR) a group of 8 lanes owns a head row and applies the head's steps one after another, as the
-//    reference's loop does; the tails and partners move through hogwild float2 atomics.
+//    sorted CSR) one thread owns a head row and applies the head's steps one after another, as the reference's
+//    loop does; the tails and partners move through hogwild float2 atomics. At most n / 8 rows are in flight.
 //  * serial (stream_mode 1): the reference's single stream per epoch (n_threads = 1) is replayed exactly. The
 //    schedule (eons / eonns) is computed in parallel; one thread walks the sampled edges in order to find where
 //    each edge's draws start in the stream (its RNG state is recorded), then the head rows run in parallel from
@@ -345,161 +345,11 @@ __device__ __forceinline__ void flush_head(const SgdDev& c, int64_t u, int dim, 
 }
 
 // ---------------------------------------------------------------------------------------------- counter mode kernels
-constexpr int kGroup = 8;
-constexpr int kNegPerRound = kGroup - 2;
-
-__device__ __forceinline__ float group_sum(float v, unsigned gmask) {
-#pragma unroll
-    for (int o = kGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o, kGroup);
-    return v;
-}
-
-// Warp kernel, loss 0, dim 2 or 3, edges sorted by head. A warp carries 4 groups of 8 lanes; each group owns one
-// head row at a time and the 4 groups advance in lockstep, one sample each per iteration. Within a sample every
-// lane runs the same code on one interaction: lanes 0-5 the negatives (negative p on lane p mod 6, in rounds when
-// there are more than 6), lane 6 the attraction towards the tail, lane 7 the mid-range partner. The head's
-// gradient is the group sum and its step is applied before the group's next sample, as in the reference's loop;
-// the tail and the partner take their steps through float2 atomics; the head's whole displacement lands with one
-// atomic when the group leaves the row.
-template <int D>
-__global__ void __launch_bounds__(kThreads) hogwild_warps_kernel(SgdDev c, const int64_t* __restrict__ eptr,
-                                                                 int epoch, float alpha, float mid_w) {
-    const int lane = threadIdx.x & 31;
-    const int gl = lane & (kGroup - 1);
-    const int gbase = lane & ~(kGroup - 1);
-    const unsigned gmask = ((1u << kGroup) - 1u) << gbase;
-    const float fepoch = (float)epoch;
-    const int64_t n_groups = (int64_t)gridDim.x * (blockDim.x / kGroup);
-    const int role = gl < kNegPerRound ? 0 : (gl == kNegPerRound ? 1 : 2);   // negative / attraction / mid-range
-    const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
-    // the common coefficient path: kernel 0 without per-node b, the same instructions on every lane
-    const bool uniform_path = c.kernel == 0 && !c.node_b;
-    const float ex = role == 1 ? c.b : c.rep_b;
-    const bool plain = role == 1 ? c.b_is_one : c.rep_b_is_one;
-    int64_t u = (int64_t)blockIdx.x * (blockDim.x / kGroup) + threadIdx.x / kGroup;
-    int64_t e1 = 0, base = 0;
-    unsigned sm = 0;
-    int nn = -1;
-    float yu[D], y0[D];
-    bool have = false;
-    if (u < c.n) { base = eptr[u] - kGroup; e1 = eptr[u + 1]; }
-    for (;;) {
-        // ---- each group moves to its next sampled edge (group-uniform control flow)
-        while (u < c.n && sm == 0) {
-            base += kGroup;
-            if (base >= e1) {
-                if (have && gl == 0 && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
-                have = false;
-                u += n_groups;
-                if (u < c.n) { base = eptr[u] - kGroup; e1 = eptr[u + 1]; }
-                continue;
-            }
-            const int64_t i = base + gl;
-            nn = i < e1 ? schedule_edge(c, i, fepoch) : -1;
-            sm = (__ballot_sync(gmask, nn >= 0) >> gbase) & ((1u << kGroup) - 1u);
-        }
-        const bool active = u < c.n;
-        if (!__any_sync(0xffffffffu, active)) break;
-        if (!active) continue;
-        // ---- one sample of the group
-        const int src = __ffs(sm) - 1;
-        sm &= sm - 1;
-        const int n_neg = __shfl_sync(gmask, nn, src, kGroup);
-        const int64_t i = base + src;
-        if (!have) {
-#pragma unroll
-            for (int d = 0; d < D; ++d) { yu[d] = c.Y[u * D + d]; y0[d] = yu[d]; }
-            have = true;
-        }
-        const int32_t v = c.tail[i];
-        const uint32_t key = sample_key(stream_seed(c.seed, epoch, (uint64_t)i));
-        float gu[D];
-#pragma unroll
-        for (int d = 0; d < D; ++d) gu[d] = 0.0f;
-        const int rounds = n_neg > kNegPerRound ? (n_neg + kNegPerRound - 1) / kNegPerRound : 1;
-        for (int r = 0; r < rounds; ++r) {
-            const int p = r * kNegPerRound + gl;
-            // this lane's partner row, or -1 when it has none this round
-            int32_t partner = -1;
-            if (role == 0) {
-                if (p < n_neg) {
-                    const int32_t k = (int32_t)below_of(counter_draw(key, p), (uint32_t)c.n);
-                    partner = k == (int32_t)u ? -1 : k;
-                }
-            } else if (r == 0) {
-                if (role == 1) {
-                    partner = v;
-                } else if (mid_w > 0.0f) {
-                    CounterDraws dr(key);
-                    if (uniform_of(dr.mid()) < c.mid_rate) {
-                        const int32_t w = mid_partner(c, (int32_t)u, v, dr);
-                        partner = w == (int32_t)u ? -1 : w;
-                    }
-                }
-            }
-            if (partner >= 0) {
-                float diff[D], d2 = 0.0f;
-#pragma unroll
-                for (int d = 0; d < D; ++d) {
-                    diff[d] = yu[d] - c.Y[(int64_t)partner * D + d];
-                    d2 = __fadd_rn(d2, __fmul_rn(diff[d], diff[d]));
-                }
-                const bool pos = d2 > 0.0f;
-                float coeff;
-                if (uniform_path) {
-                    // every lane evaluates the same few instructions: d2^ex through log2 / exp2 and fast
-                    // divisions (a few ulp; d2 = 0 gives pw = 0, its coefficient is masked below)
-                    const float pw_e = exp2f(ex * __log2f(d2));
-                    const float pw = plain ? d2 : pw_e;
-                    const float att = __fdividef(-c.exaggeration * 2.0f * c.a * c.b * pw, d2 * (c.a * pw + 1.0f));
-                    const float rep = __fdividef(c.two_b, (0.001f + d2) * (c.rep_a * pw + 1.0f));
-                    coeff = role == 0 ? rep : (role == 1 ? att : -mid_w);
-                } else if (role == 0) {
-                    coeff = pos ? repulsion_coeff(c, d2, (int32_t)u) : 0.0f;
-                } else if (role == 1) {
-                    const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
-                    const float pw_v = (c.b_is_one && !c.node_b) ? d2 : (pos ? powf(d2, b_uv) : 0.0f);
-                    coeff = pos ? attraction_coeff(c, d2, b_uv, pw_v) : 0.0f;
-                } else {
-                    coeff = -mid_w;
-                }
-                if (!pos && role != 2) coeff = 0.0f;
-                float gk[D];
-#pragma unroll
-                for (int d = 0; d < D; ++d) { const float g = coeff * diff[d]; gu[d] += g; gk[d] = -g; }
-                if (role == 0 && !pos) {
-#pragma unroll
-                    for (int d = 0; d < D; ++d)
-                        gu[d] += (uniform_of(counter_draw(key, kJitterDraw + 64 * p + d)) - 0.5f) * jit;
-                }
-                const bool moves = ((role == 1 && pos) || role == 2) && partner >= c.n_fixed;
-                if (moves) HogwildSink().template apply<D>(c, partner, gk, alpha, D);
-            }
-        }
-#pragma unroll
-        for (int d = 0; d < D; ++d) gu[d] = group_sum(gu[d], gmask);
-        if (u >= c.n_fixed) {
-            float step[D];
-            if (c.optimizer == 1) {
-                // lazy Adam of the head: one lane updates the state, the step is broadcast
-                if (gl == 0) make_step<D>(c, gu, alpha, u, D, step);
-#pragma unroll
-                for (int d = 0; d < D; ++d) step[d] = __shfl_sync(gmask, step[d], 0, kGroup);
-            } else {
-                make_step<D>(c, gu, alpha, u, D, step);
-            }
-#pragma unroll
-            for (int d = 0; d < D; ++d) yu[d] += step[d];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------------------------- list kernels
 // The counter mode's fast path (loss 0, dim 2 or 3, edges sorted by head) runs an epoch as two kernels:
-// compact_schedule_kernel writes each row's sampled edges as a compact list, then hogwild_list_kernel gives each
-// row to one thread, which does the row's samples in order, so the head's steps follow one another as in the
-// reference's loop. A sample first gathers what it reads (its list entry, tail, draws, the positions of its tail
-// and negatives), then computes.
+// schedule16_kernel runs the schedule of every edge (one thread per edge) and records each edge's negatives, or
+// "not sampled"; hogwild_list_kernel gives each thread a run of consecutive rows, and the thread does each row's
+// sampled edges in order, so the head's steps follow one another as in the reference's loop. A sample first
+// gathers what it reads (tail, draws, the positions of its tail and negatives), then computes.
 constexpr int kNegBatch = 6;   // n_neg is 4-6 for almost every sample (its long-run mean is the rate, 5)
 
 template <int D>
@@ -617,92 +467,67 @@ __device__ __forceinline__ void compute_sample(const SgdDev& c, int64_t u, const
     if (u >= c.n_fixed) local_step<D>(c, yu, gu, alpha, u, D);
 }
 
-// Schedule of an epoch as per-row compact lists. A warp takes a run of whole rows and walks their edges 32 at a
-// time, across row boundaries (coalesced, every lane busy): it runs the schedule of each edge (eons / eonns advance
-// as in the reference) and writes the sampled ones, in order, at the start of their row's own edge range:
-// samp[eptr[u] + j] = edge, nneg[...] = its negatives; rcnt[u] = the row's count. A sampled edge's rank in its row
-// is the count of sampled edges of the same row in lower lanes (the row's lanes form a run, the heads being
-// sorted) plus those of the row in the warp's previous chunks. No global scan is needed, since a row's list fits in its own range.
-__global__ void __launch_bounds__(kThreads) compact_schedule_kernel(SgdDev c, const int64_t* __restrict__ eptr,
-                                                                    int epoch, int64_t rows_per_warp,
-                                                                    int32_t* __restrict__ samp,
-                                                                    int32_t* __restrict__ nneg,
-                                                                    int32_t* __restrict__ rcnt) {
-    const int lane = threadIdx.x & 31;
-    const unsigned lower = (1u << lane) - 1u;
+// Schedule of an epoch, one thread per edge (coalesced): eons / eonns advance as in the reference, cnt16[i] = the
+// edge's negatives this epoch, or 0xFFFF when it is not sampled. n_neg = (epoch - eonn) / (eps / rate) with
+// eps >= 1 stays below rate x epochs, far under 65535 for the rates and epoch counts the reference uses.
+__global__ void __launch_bounds__(kThreads) schedule16_kernel(SgdDev c, int epoch, uint16_t* __restrict__ cnt16) {
     const float fepoch = (float)epoch;
-    const int64_t r0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * rows_per_warp;
-    if (r0 >= c.n) return;
-    const int64_t r1 = r0 + rows_per_warp < c.n ? r0 + rows_per_warp : c.n;
-    for (int64_t u = r0 + lane; u < r1; u += 32) rcnt[u] = 0;   // rows without edges keep 0
-    __syncwarp();
-    const int64_t es = eptr[r0], ee = eptr[r1];
-    int32_t carry_row = -1;   // the row that continues from the previous chunk, and its count so far
-    int carry = 0;
-    for (int64_t base = es; base < ee; base += 32) {
-        const int64_t i = base + lane;
-        const bool valid = i < ee;
-        const int32_t h = valid ? c.head[i] : -1;
-        const int nn = valid ? schedule_edge(c, i, fepoch) : -1;
-        const unsigned flags = __ballot_sync(0xffffffffu, nn >= 0);
-        // heads are sorted, so the lanes of a row form a run: [its start lane, the next start lane)
-        const int32_t h_prev = __shfl_up_sync(0xffffffffu, h, 1);
-        const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || h != h_prev);
-        const unsigned upto = lane == 31 ? 0xffffffffu : (2u << lane) - 1u;   // lanes <= this one
-        const int run0 = 31 - __clz(starts & upto);
-        const unsigned after = starts & ~upto;
-        const int run1 = after ? __ffs(after) - 1 : 32;
-        const unsigned peers = (unsigned)((1ull << run1) - (1ull << run0));
-        const int before = (h == carry_row) ? carry : 0;
-        if (nn >= 0) {
-            const int64_t slot = eptr[h] + before + __popc(peers & flags & lower);
-            samp[slot] = (int32_t)i;
-            nneg[slot] = nn;
-        }
-        const int total = before + __popc(peers & flags);
-        int32_t nh = -1;   // head of the first edge of the next chunk
-        if (lane == 0 && base + 32 < ee) nh = c.head[base + 32];
-        nh = __shfl_sync(0xffffffffu, nh, 0);
-        const bool last_of_row = lane == 31 - __clz(peers);
-        if (valid && last_of_row && !(lane == 31 && nh == h)) rcnt[h] = total;
-        const int32_t h31 = __shfl_sync(0xffffffffu, h, 31);
-        const int t31 = __shfl_sync(0xffffffffu, total, 31);
-        if (h31 >= 0 && nh == h31) { carry_row = h31; carry = t31; } else { carry_row = -1; carry = 0; }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges; i += (int64_t)gridDim.x * blockDim.x) {
+        const int nn = schedule_edge(c, i, fepoch);
+        cnt16[i] = nn < 0 ? (uint16_t)0xFFFF : (uint16_t)nn;
     }
 }
 
+// One thread per run of consecutive rows (rows_per_thread of them): for each row, 64 edges at a time, the
+// sampled edges become a bit mask and are done in edge order. A thread moving through several rows keeps the
+// warps' threads busy for about the same number of samples (the sum over 8 or so rows varies less than one row's
+// count). The head's displacement lands with one atomic when the thread leaves the row.
 template <int D, bool FAST, bool REP1, bool B1>
 __global__ void __launch_bounds__(kThreads, 4) hogwild_list_kernel(SgdDev c, const int64_t* __restrict__ eptr,
-                                                                const int32_t* __restrict__ samp,
-                                                                const int32_t* __restrict__ nneg,
-                                                                const int32_t* __restrict__ rcnt, int epoch,
-                                                                float alpha, float mid_w) {
+                                                                   const uint16_t* __restrict__ cnt16, int epoch,
+                                                                   float alpha, float mid_w, int64_t rows_per_thread) {
     const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < c.n; u += (int64_t)gridDim.x * blockDim.x) {
-        const int cnt = rcnt[u];
-        if (cnt == 0) continue;
-        const int64_t e0 = eptr[u];
+    const int64_t u0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * rows_per_thread;
+    const int64_t uend = u0 + rows_per_thread < c.n ? u0 + rows_per_thread : c.n;
+    for (int64_t u = u0; u < uend; ++u) {
+        const int64_t e0 = eptr[u], e1 = eptr[u + 1];
         float yu[D], y0[D];
-        load_pos<D>(c.Y, u, yu);
+        bool have = false;
+        for (int64_t w0 = e0; w0 < e1; w0 += 64) {
+            // sampled edges of this 64-edge window of the row, as a bit mask
+            const int m = e1 - w0 < 64 ? (int)(e1 - w0) : 64;
+            unsigned long long mask = 0ull;
+            for (int k = 0; k < m; ++k)
+                if (cnt16[w0 + k] != 0xFFFF) mask |= 1ull << k;
+            while (mask) {
+                const int k = __ffsll((long long)mask) - 1;
+                mask &= mask - 1ull;
+                if (!have) {
+                    load_pos<D>(c.Y, u, yu);
 #pragma unroll
-        for (int d = 0; d < D; ++d) y0[d] = yu[d];
-        for (int j = 0; j < cnt; ++j) {
-            Fetched<D> f;
-            fetch_sample<D>(c, samp[e0 + j], nneg[e0 + j], epoch, f);
-            compute_sample<D, FAST, REP1, B1>(c, u, f, alpha, mid_w, jit, yu);
+                    for (int d = 0; d < D; ++d) y0[d] = yu[d];
+                    have = true;
+                }
+                Fetched<D> f;
+                fetch_sample<D>(c, w0 + k, (int)cnt16[w0 + k], epoch, f);
+                compute_sample<D, FAST, REP1, B1>(c, u, f, alpha, mid_w, jit, yu);
+            }
         }
-        if (u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+        if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
     }
 }
 
 template <int D, bool FAST>
-void launch_list(const SgdDev& c, int blocks, const int64_t* eptr, const int32_t* samp, const int32_t* nneg,
-                 const int32_t* rcnt, int epoch, float alpha, float mid_w, cudaStream_t s) {
+void launch_list(const SgdDev& c, int blocks, const int64_t* eptr, const uint16_t* cnt16, int epoch, float alpha,
+                 float mid_w, cudaStream_t s) {
+    const int64_t threads = (int64_t)blocks * kThreads;
+    const int64_t rpt = (c.n + threads - 1) / threads;
+    blocks = (int)((c.n + rpt * kThreads - 1) / (rpt * kThreads));
     const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
-    if (rep1 && b1) hogwild_list_kernel<D, FAST, true, true><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
-    else if (rep1) hogwild_list_kernel<D, FAST, true, false><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
-    else if (b1) hogwild_list_kernel<D, FAST, false, true><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
-    else hogwild_list_kernel<D, FAST, false, false><<<blocks, kThreads, 0, s>>>(c, eptr, samp, nneg, rcnt, epoch, alpha, mid_w);
+    if (rep1 && b1) hogwild_list_kernel<D, FAST, true, true><<<blocks, kThreads, 0, s>>>(c, eptr, cnt16, epoch, alpha, mid_w, rpt);
+    else if (rep1) hogwild_list_kernel<D, FAST, true, false><<<blocks, kThreads, 0, s>>>(c, eptr, cnt16, epoch, alpha, mid_w, rpt);
+    else if (b1) hogwild_list_kernel<D, FAST, false, true><<<blocks, kThreads, 0, s>>>(c, eptr, cnt16, epoch, alpha, mid_w, rpt);
+    else hogwild_list_kernel<D, FAST, false, false><<<blocks, kThreads, 0, s>>>(c, eptr, cnt16, epoch, alpha, mid_w, rpt);
 }
 
 // Row kernel (any dim, any loss): one thread owns a head row and walks it in order with counter draws.
@@ -927,19 +752,13 @@ void hogwild_epoch(const SgdDev& c, SgdWork& w, const int64_t* eptr, int epoch, 
                    cudaStream_t s) {
     const int64_t cap = max_in_flight(c);
     if (eptr && c.loss == 0 && (D == 2 || D == 3)) {
-        int32_t* samp = w.samp.as<int32_t>();
-        int32_t* nneg = w.nneg.as<int32_t>();
-        int32_t* rcnt = w.rcnt.as<int32_t>();
-        const int64_t warps = (int64_t)kNumSMs * 64;   // one resident wave of warps
-        const int64_t rows_per_warp = std::max<int64_t>(1, (c.n + warps - 1) / warps);
-        const int64_t n_warps = (c.n + rows_per_warp - 1) / rows_per_warp;
-        compact_schedule_kernel<<<(int)((n_warps + kThreads / 32 - 1) / (kThreads / 32)), kThreads, 0, s>>>(
-            c, eptr, epoch, rows_per_warp, samp, nneg, rcnt);
+        uint16_t* cnt16 = w.samp.as<uint16_t>();
+        schedule16_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c, epoch, cnt16);
         MGB_LAUNCH_CHECK();
         const int blocks = (int)std::min<int64_t>(blocks_for(c.n, kThreads, 8), (cap + kThreads - 1) / kThreads);
         constexpr int DD = D == 0 ? 2 : D;
-        if (c.kernel == 0 && !c.node_b) launch_list<DD, true>(c, blocks, eptr, samp, nneg, rcnt, epoch, alpha, mid_w, s);
-        else launch_list<DD, false>(c, blocks, eptr, samp, nneg, rcnt, epoch, alpha, mid_w, s);
+        if (c.kernel == 0 && !c.node_b) launch_list<DD, true>(c, blocks, eptr, cnt16, epoch, alpha, mid_w, s);
+        else launch_list<DD, false>(c, blocks, eptr, cnt16, epoch, alpha, mid_w, s);
     } else if (eptr) {
         const int blocks = (int)std::min<int64_t>(blocks_for(c.n, kThreads), (cap + kThreads - 1) / kThreads);
         hogwild_rows_kernel<D><<<blocks, kThreads, 0, s>>>(c, eptr, epoch, alpha, mid_w);
@@ -1013,9 +832,7 @@ void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha
     const int64_t* eptr = row_pointers(c, w, s);
     if (stream_mode == 0) {
         if (eptr && c.loss == 0 && (c.dim == 2 || c.dim == 3)) {
-            w.samp.ensure(sizeof(int32_t) * std::max<int64_t>(c.n_edges, 1));
-            w.nneg.ensure(sizeof(int32_t) * std::max<int64_t>(c.n_edges, 1));
-            w.rcnt.ensure(sizeof(int32_t) * std::max<int64_t>(c.n, 1));
+            w.samp.ensure(sizeof(uint16_t) * std::max<int64_t>(c.n_edges, 1));
         }
         for (int e = e0; e < e1; ++e) {
             float alpha, mid_w;

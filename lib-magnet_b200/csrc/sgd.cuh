@@ -25,7 +25,7 @@ struct SgdDev {
 // device scratch of the serial stream mode
 struct SgdWork {
     DevBuf cnt, state, delta, eptr, flag;
-    DevBuf samp, nneg, rcnt;   // per-row compact lists of the epoch's sampled edges (counter mode)
+    DevBuf samp;               // the epoch's per-edge negatives counts (counter mode fast path)
 };
 
 void sgd_sched(const SgdDev& c, int epoch, int e0, int e1, float alpha0, float alpha1, float mid_w0, float mid_w1,

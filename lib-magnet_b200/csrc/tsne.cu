@@ -243,8 +243,35 @@ __global__ void __launch_bounds__(kThreads) loop_iter_kernel(const float2* __res
     const int64_t groups = (int64_t)gridDim.x * (blockDim.x / T);
     for (int64_t i = (int64_t)blockIdx.x * (blockDim.x / T) + threadIdx.x / T; i < n; i += groups) {
         const float2 yi = Ycur[i];
+        // the gather's loads (which need only y_i) and the step's state are issued first, so that their latency
+        // overlaps the attraction's chain of CSR and neighbour loads; the stencil nodes are split over the row's
+        // lanes (node q on lane q mod T) and summed by shuffles (src/fftconv.cpp:211-222)
+        int bx, by;
+        float wx[NI], wy[NI];
+        locate<NI>(yi.x, yi.y, xmin, ymin, width, inv_w, nb, bx, by, wx, wy);
+        constexpr int kPer = (NI * NI + T - 1) / T;
+        float gw[kPer], g1[kPer], g2[kPer], g3[kPer];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) {
+            const int q = lg + r * T;
+            gw[r] = 0.f; g1[r] = 0.f; g2[r] = 0.f; g3[r] = 0.f;
+            if (q < NI * NI) {
+                const int a = q / NI, b = q - a * NI;
+                float wa = 0.f, wb = 0.f;
+#pragma unroll
+                for (int t = 0; t < NI; ++t) { if (t == a) wa = wx[t]; if (t == b) wb = wy[t]; }
+                gw[r] = wa * wb;
+                const size_t node = (size_t)(bx * NI + a) * pitchP + (size_t)by * NI + b;
+                g1[r] = __ldg(&phi[plane + node]);
+                g2[r] = __ldg(&phi[2 * plane + node]);
+                g3[r] = __ldg(&phi[3 * plane + node]);
+            }
+        }
+        float2 u = make_float2(0.f, 0.f), gn = make_float2(0.f, 0.f);
+        if (lg == 0) { u = U[i]; gn = G[i]; }
         float ax = 0.f, ay = 0.f;
         const int32_t e1 = ip[i + 1];
+#pragma unroll 4
         for (int32_t e = ip[i] + lg; e < e1; e += T) {
             const float2 yj = __ldg(&Ycur[ix[e]]);
             const float dx = yi.x - yj.x, dy = yi.y - yj.y;
@@ -256,23 +283,9 @@ __global__ void __launch_bounds__(kThreads) loop_iter_kernel(const float2* __res
             ax += __shfl_xor_sync(gmask, ax, o, T);
             ay += __shfl_xor_sync(gmask, ay, o, T);
         }
-        // gather of the potentials at the NI x NI stencil (src/fftconv.cpp:211-222), the nodes split over the
-        // row's lanes (node q on lane q mod T) and summed by shuffles
-        int bx, by;
-        float wx[NI], wy[NI];
-        locate<NI>(yi.x, yi.y, xmin, ymin, width, inv_w, nb, bx, by, wx, wy);
         float p1 = 0.f, p2 = 0.f, p3 = 0.f;
-        for (int q = lg; q < NI * NI; q += T) {
-            const int a = q / NI, b = q - a * NI;
-            float wa = 0.f, wb = 0.f;
 #pragma unroll
-            for (int t = 0; t < NI; ++t) { if (t == a) wa = wx[t]; if (t == b) wb = wy[t]; }
-            const float w = wa * wb;
-            const size_t node = (size_t)(bx * NI + a) * pitchP + (size_t)by * NI + b;
-            p1 += w * __ldg(&phi[plane + node]);
-            p2 += w * __ldg(&phi[2 * plane + node]);
-            p3 += w * __ldg(&phi[3 * plane + node]);
-        }
+        for (int r = 0; r < kPer; ++r) { p1 += gw[r] * g1[r]; p2 += gw[r] * g2[r]; p3 += gw[r] * g3[r]; }
 #pragma unroll
         for (int o = T / 2; o > 0; o >>= 1) {
             p1 += __shfl_xor_sync(gmask, p1, o, T);
@@ -281,7 +294,6 @@ __global__ void __launch_bounds__(kThreads) loop_iter_kernel(const float2* __res
         }
         if (lg == 0) {
             const float fx = __fsub_rn(__fmul_rn(p1, yi.x), p2), fy = __fsub_rn(__fmul_rn(p1, yi.y), p3);
-            float2 u = U[i], gn = G[i];
             const float gx_ = __fsub_rn(__fmul_rn(rho, ax), __fmul_rn(fx, inv_sumQ));
             const float gy_ = __fsub_rn(__fmul_rn(rho, ay), __fmul_rn(fy, inv_sumQ));
             const float nx = step_coord(yi.x, u.x, gn.x, gx_, s.lr, mom);
