@@ -83,7 +83,8 @@ void validate_csr_host(const int32_t* ip, const int32_t* ix, int64_t nnz, int64_
     if (!ip || is_device_ptr(ip)) return;
     if (n_cols < 0) n_cols = n;
     require(ip[0] == 0, std::string(what) + ": indptr[0] must be 0");
-    for (int64_t i = 0; i < n; ++i) require(ip[i + 1] >= ip[i], std::string(what) + ": indptr must be non-decreasing");
+    for (int64_t i = 0; i < n; ++i)
+        if (ip[i + 1] < ip[i]) require(false, std::string(what) + ": indptr must be non-decreasing");
     require((int64_t)ip[n] == nnz, std::string(what) + ": indices must have indptr[n] entries");
     if (ix && !is_device_ptr(ix))
         for (int64_t j = 0; j < nnz; ++j) require(ix[j] >= 0 && ix[j] < n_cols, "column index out of range");

@@ -23,6 +23,10 @@ struct Error : std::runtime_error {
 inline void require(bool ok, const std::string& msg) {
     if (!ok) throw Error(MG_ERR_ARGUMENT, msg);
 }
+// the message is built only on failure (the host-side checks run once per edge on host arrays)
+inline void require(bool ok, const char* msg) {
+    if (!ok) throw Error(MG_ERR_ARGUMENT, msg);
+}
 
 #define MGB_CUDA(call)                                                                                    \
     do {                                                                                                  \
