@@ -56,7 +56,6 @@ void RepBuffers::alloc(int Nmax_, int Mmax_, int ni_) {
     // The in-place engine runs when the largest length has a plan: an FFTConv2D object computes at M = Mmax only,
     // and the device loop takes its lengths from the table below, which then holds planned lengths only.
     fft3::Plan pmax;
-    use2 = false;
     use3 = fft3::make_plan(Mmax, pmax);
     fft3_build_plans(plans3, Mmax, Mp3max);
     if (use3) fft3_prepare(Mp3max);
@@ -498,10 +497,6 @@ void ensure_fft_attrs() {
 }
 
 void rep_convolve(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEvent_t* ev) {
-    if (b.use2) {
-        rep_convolve2(g, b, n, s, ev);
-        return;
-    }
     if (b.use3) {
         rep_row_fwd3(g, b, s);
         if (ev) MGB_CUDA(cudaEventRecord(ev[0], s));
@@ -544,10 +539,6 @@ void rep_prepare_device_spectra(RepBuffers& b) {
 void rep_update_spectra(GridDesc* g, RepBuffers& b, float dof, cudaStream_t s) {
     const int Pa = b.Mmax / 2 + 1;
     require(b.Rt.p != nullptr, "rep_prepare_device_spectra must run first");
-    if (b.use2) {
-        rep_update_spectra2(g, b, dof, s);
-        return;
-    }
     const size_t smem = fft_smem(b.Mmax);
     spec_rows_kernel<<<fft_blocks(Pa), kFftThreads, smem, s>>>(g, b.Rt.as<float2>(), Pa, b.Mhmax, b.tw.as<float2>(),
                                                                 b.ni, (double)dof);

@@ -35,9 +35,8 @@ struct GridDesc {
 
 struct RepBuffers {
     int Nmax = 0, Mmax = 0, Mhmax = 0, Npmax = 0, ni = 3;
-    DevBuf W, WhT, PhT, phi, Kt, Rt, tw, zpart, fft_len_table, bbox_part, mean_part, plans;
+    DevBuf W, WhT, PhT, phi, Kt, Rt, tw, zpart, fft_len_table, bbox_part, mean_part;
     int max_bbox_blocks = 0;
-    bool use2 = false;        // the register-tiled FFT engine (fftrep2.cu) holds this Mmax
     DevBuf plans3;            // in-place engine (fft3.cuh) plans, indexed by M
     int Mp3max = 0;           // its largest padded length up to Mmax
     bool use3 = false;        // the in-place column pass (fftrep3.cu) runs every length these buffers see
@@ -74,12 +73,6 @@ void rep_col3(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s);
 void rep_row_fwd3(GridDesc* g, RepBuffers& b, cudaStream_t s);
 void rep_row_inv3(GridDesc* g, RepBuffers& b, cudaStream_t s);
 
-// register-tiled engine (fftrep2.cu)
-bool fft2_fits(int Mmax);
-void fft2_build_plans(DevBuf& table, int Mmax);
-void ensure_fft2_attrs();
-void rep_convolve2(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEvent_t* ev);
-void rep_update_spectra2(GridDesc* g, RepBuffers& b, float dof, cudaStream_t s);
 
 // the whole t-SNE iteration pieces (tsne.cu)
 struct TsneDev;

@@ -70,7 +70,6 @@ struct ScratchView {
     RepBuffers rb;
     explicit ScratchView(unsigned char* base, int ni) {
         rb.Nmax = kNoallocMaxM; rb.Mmax = kNoallocMaxM; rb.Mhmax = kMh; rb.Npmax = kNp; rb.ni = ni;
-        rb.use2 = false;
         lend(rb.W, base + kWOff, kWBytes);
         lend(rb.WhT, base + kWhOff, kWhBytes);
         lend(rb.PhT, base + kPhOff, kPhBytes);

@@ -81,3 +81,35 @@ def test_grid_too_large_raises(mg):
     conv = mg.FFTConv2D(120, 3)
     with pytest.raises(RuntimeError, match="grid larger than the buffer"):
         conv.compute(np.zeros((10, 2), np.float32), 0.0, 0.0, 0.7, 60)
+
+
+def spectra_on_torus(M, n_boxes, width, ni, dof=1.0):
+    """the kernel spectra of FFTRepulsion2D._kernels (magnet/tsne.py:48-71) on a given M torus (M >= 2N): the
+    convolution of the N live nodes is the same for every such M"""
+    import scipy.fft as fft
+    delta = width / ni
+    off = np.arange(M)
+    off = np.where(off <= M // 2, off, off - M).astype(np.float64) * delta
+    base = 1.0 + (off[:, None] ** 2 + off[None, :] ** 2) / dof
+    K1 = (base ** (-dof)).astype(np.float32)
+    K2 = (base ** (-dof - 1.0)).astype(np.float32)
+    h = lambda K: np.ascontiguousarray(np.ascontiguousarray(fft.rfft2(K), dtype=np.complex64).real)
+    return h(K1), h(K2)
+
+
+# FFT sides covering the in-place engine's plan shapes: two stages (120 = 8 x 15), three with an even last radix
+# and padding (512 = 8 x 8 x 8, 1000 = 10 x 10 x 10), three with an odd last radix (4320 = 18 x 16 x 15), four
+# stages (2187 = 9 x 9 x 9 x 3; 8192 = 16 x 16 x 2 x 16, padded), and a 5-smooth side without a plan, which runs
+# the one-radix engine (3125 = 5^5)
+@pytest.mark.parametrize("M", [120, 512, 1000, 2187, 3125, 4320, 8192])
+def test_fft_sides_against_fp64(mg, M):
+    ni, nb, width = 3, 20, 0.7
+    rng = np.random.default_rng(M)
+    Y = rng.uniform(0.01, nb * width - 0.01, (3000, 2)).astype(np.float32)
+    K1, K2 = spectra_on_torus(M, nb, width, ni)
+    conv = mg.FFTConv2D(M, ni)
+    conv.set_kernels(K1, K2)
+    sq, F = conv.compute(Y, 0.0, 0.0, width, nb)
+    sq64, F64 = O.fft_repulsion_fp64(Y, 0.0, 0.0, width, nb, n_interp=ni)
+    assert abs(sq - sq64) / sq64 < TOL
+    assert np.linalg.norm(F - F64) / np.linalg.norm(F64) < TOL
