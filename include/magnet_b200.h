@@ -156,7 +156,7 @@ typedef struct {
     uint64_t seed;
     int n_threads;               /* accepted for signature parity; the device decides its own parallelism */
     int parallel;                /* 0 hogwild (reference), accepted values as the reference */
-    int stream_mode;             /* 0 = counter-based stream per (epoch, edge) (fast, default);
+    int stream_mode;             /* 0 = counter-based draws per (epoch, edge, index) (fast, default);
                                     1 = the reference's single stream per epoch replayed exactly (serial mode),
                                         updates from an epoch snapshot in fixed point: deterministic */
 } mg_layout_args;

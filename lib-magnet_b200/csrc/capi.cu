@@ -12,6 +12,7 @@
 #include <cmath>
 #include <algorithm>
 #include <atomic>
+#include <thread>
 
 namespace mgb {
 
@@ -77,17 +78,46 @@ bool any_host(std::initializer_list<const void*> ptrs) {
     return false;
 }
 
+// The first i in [0, count) where ok(i) fails, or -1: large ranges are split over the host's cores (the checks of
+// host arrays run once per element and call); each chunk stops at its own first failure and the smallest wins.
+template <class F>
+int64_t first_failure(int64_t count, F ok) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (count < (1 << 20) || hw == 1) {
+        for (int64_t i = 0; i < count; ++i)
+            if (!ok(i)) return i;
+        return -1;
+    }
+    const int64_t chunk = (count + hw - 1) / hw;
+    std::vector<int64_t> first(hw, -1);
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < hw; ++t) {
+        const int64_t b = t * chunk, e = std::min<int64_t>(count, b + chunk);
+        if (b >= e) break;
+        pool.emplace_back([&, t, b, e] {
+            for (int64_t i = b; i < e; ++i)
+                if (!ok(i)) { first[t] = i; return; }
+        });
+    }
+    for (auto& th : pool) th.join();
+    for (int64_t f : first)
+        if (f >= 0) return f;   // chunks are in index order
+    return -1;
+}
+template <class F>
+bool all_of_range(int64_t count, F ok) { return first_failure(count, ok) < 0; }
+
 // validate_csr of src/layout.hpp:21-32 (host arrays only; device arrays are the caller's responsibility)
 void validate_csr_host(const int32_t* ip, const int32_t* ix, int64_t nnz, int64_t n, int64_t n_cols,
                        const char* what) {
     if (!ip || is_device_ptr(ip)) return;
     if (n_cols < 0) n_cols = n;
     require(ip[0] == 0, std::string(what) + ": indptr[0] must be 0");
-    for (int64_t i = 0; i < n; ++i)
-        if (ip[i + 1] < ip[i]) require(false, std::string(what) + ": indptr must be non-decreasing");
+    if (!all_of_range(n, [&](int64_t i) { return ip[i + 1] >= ip[i]; }))
+        require(false, std::string(what) + ": indptr must be non-decreasing");
     require((int64_t)ip[n] == nnz, std::string(what) + ": indices must have indptr[n] entries");
     if (ix && !is_device_ptr(ix))
-        for (int64_t j = 0; j < nnz; ++j) require(ix[j] >= 0 && ix[j] < n_cols, "column index out of range");
+        require(all_of_range(nnz, [&](int64_t j) { return ix[j] >= 0 && ix[j] < n_cols; }), "column index out of range");
 }
 
 // sum of P in FP64: per-block partials, the last block adds them in block order (deterministic)
@@ -438,17 +468,23 @@ SgdDev prepare_sgd(const mg_layout_args& A, cudaStream_t s) {
     if (A.stream_mode == 1 && A.optimizer == 1)
         throw Error(MG_ERR_NOT_SUPPORTED, "the serial stream mode supports the sgd optimizer only");
     if (A.head && !is_device_ptr(A.head)) {
-        for (int64_t i = 0; i < E; ++i) {
-            require(A.head[i] >= 0 && A.head[i] < n && A.tail[i] >= 0 && A.tail[i] < n, "edge index out of range");
-            require(A.epochs_per_sample[i] > 0.0f, "epochs_per_sample must be positive");
+        // the reference's per-edge checks (src/layout.cpp:385-388); the first failing edge names the message
+        const int32_t* hd = A.head; const int32_t* tl = A.tail; const float* ep = A.epochs_per_sample;
+        const auto edge_ok = [&](int64_t i) { return hd[i] >= 0 && hd[i] < n && tl[i] >= 0 && tl[i] < n; };
+        const int64_t f = first_failure(E, [&](int64_t i) { return edge_ok(i) && ep[i] > 0.0f; });
+        if (f >= 0) {
+            require(edge_ok(f), "edge index out of range");
+            require(false, "epochs_per_sample must be positive");
         }
     }
     const bool adam = A.optimizer == 1;
     if (adam) require(A.adam_m && A.adam_v && A.adam_t, "Adam state arrays have the wrong shape");
     const bool has_pairs = A.mid_pairs != nullptr && A.n_mid > 0;
-    if (has_pairs && !is_device_ptr(A.mid_pairs))
-        for (int64_t i = 0; i < n * A.n_mid; ++i)
-            require(A.mid_pairs[i] >= 0 && A.mid_pairs[i] < n, "mid_pairs index out of range");
+    if (has_pairs && !is_device_ptr(A.mid_pairs)) {
+        const int32_t* mp = A.mid_pairs;
+        require(all_of_range(n * A.n_mid, [&](int64_t i) { return mp[i] >= 0 && mp[i] < n; }),
+                "mid_pairs index out of range");
+    }
     const bool has_jumps = A.jump_indptr != nullptr && A.mid_jump > 0.0f;
     if (has_jumps) validate_csr_host(A.jump_indptr, A.jump_indices, A.jump_nnz, n, -1, "jump graph");
     const bool walks = has_jumps || !has_pairs;
