@@ -422,6 +422,26 @@ void launch_iter_t(TsneDev& d, cudaStream_t st) {
         d.mean_part.as<double2>());
 }
 
+// resident blocks of the iteration kernel for (NI, T): the grid is one resident wave (the kernel loops over
+// rows), so no second partial wave idles the device before the last-block reduction
+template <int NI, int T>
+int iter_blocks_t() {
+    int per_sm = 0;
+    MGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, loop_iter_kernel<NI, T>, kThreads, 0));
+    return std::max(1, per_sm) * kNumSMs;
+}
+template <int NI>
+int iter_blocks_ni(int tpr) {
+    switch (tpr) {
+        case 1: return iter_blocks_t<NI, 1>();
+        case 2: return iter_blocks_t<NI, 2>();
+        case 4: return iter_blocks_t<NI, 4>();
+        case 8: return iter_blocks_t<NI, 8>();
+        case 16: return iter_blocks_t<NI, 16>();
+        default: return iter_blocks_t<NI, 32>();
+    }
+}
+
 template <int NI>
 void launch_iter_ni(TsneDev& d, cudaStream_t st) {
     switch (d.tpr) {
@@ -540,7 +560,18 @@ void TsneDev::init(const int32_t* ip_h, const int32_t* ix_h, const float* P_h, i
     gdesc.ensure(sizeof(GridDesc));
     MGB_CUDA(cudaMemsetAsync(gdesc.p, 0, sizeof(GridDesc), st));
     blocks_bbox = grid_blocks(n, kThreads, 4);
-    blocks_iter = grid_blocks(n, kThreads / tpr, 8);
+    int resident = 0;
+    switch (s.ni) {
+        case 1: resident = iter_blocks_ni<1>(tpr); break;
+        case 2: resident = iter_blocks_ni<2>(tpr); break;
+        case 3: resident = iter_blocks_ni<3>(tpr); break;
+        case 4: resident = iter_blocks_ni<4>(tpr); break;
+        case 5: resident = iter_blocks_ni<5>(tpr); break;
+        case 6: resident = iter_blocks_ni<6>(tpr); break;
+        case 7: resident = iter_blocks_ni<7>(tpr); break;
+        default: resident = iter_blocks_ni<8>(tpr); break;
+    }
+    blocks_iter = std::min(grid_blocks(n, kThreads / tpr, 8), resident);
     bbox_part.ensure(sizeof(BBox) * blocks_bbox);
     mean_part.ensure(sizeof(double2) * blocks_iter);
     if (graph && signature() != graph_sig) { cudaGraphExecDestroy(graph); graph = nullptr; }
