@@ -190,12 +190,15 @@ py::tuple layout_schedule(py::object Y, py::object head, py::object tail, py::ob
                           py::object eonns, int epoch, int epoch_start, int epoch_end, float alpha0, float alpha1,
                           float mid_w0, float mid_w1, float negative_sample_rate, int loss, float mid_rate,
                           int walk_len, int64_t n_fixed, py::object mid_pairs, py::object indptr, py::object indices,
-                          uint64_t seed, int stream_mode) {
+                          uint64_t seed, int stream_mode, py::object walk_lens, py::object jump_indptr,
+                          py::object jump_indices, float mid_jump) {
     auto y = view<float>(Y);
     auto h = view<int32_t>(head), t = view<int32_t>(tail);
     auto e = view<float>(eps), en = view<float>(eons), enn = view<float>(eonns);
     auto mp = view<int32_t>(mid_pairs);
     auto ip = view<int32_t>(indptr), ix = view<int32_t>(indices);
+    auto wl = view<int32_t>(walk_lens);
+    auto jp = view<int32_t>(jump_indptr), jx = view<int32_t>(jump_indices);
     const int64_t E = h.size();
     mg_layout_args A;
     mg_layout_args_default(&A);
@@ -207,6 +210,9 @@ py::tuple layout_schedule(py::object Y, py::object head, py::object tail, py::ob
     A.mid_rate = mid_rate; A.walk_len = walk_len; A.n_fixed = n_fixed; A.seed = seed; A.stream_mode = stream_mode;
     A.mid_pairs = mp.size() > 0 ? mp.ptr : nullptr; A.n_mid = mp.size() > 0 ? (int)mp.dim(1) : 0;
     A.indptr = ip.size() > 0 ? ip.ptr : nullptr; A.indices = ix.size() > 0 ? ix.ptr : nullptr; A.graph_nnz = ix.size();
+    A.walk_lens = wl.size() > 0 ? wl.ptr : nullptr;
+    A.jump_indptr = jp.size() > 0 ? jp.ptr : nullptr; A.jump_indices = jx.size() > 0 ? jx.ptr : nullptr;
+    A.jump_nnz = jx.size(); A.mid_jump = mid_jump;
     const int64_t cap = E * ((int64_t)negative_sample_rate + 2) + 64;
     py::array_t<uint8_t> sampled(E);
     py::array_t<int32_t> n_neg(E), mid(E), negs(cap);
@@ -251,7 +257,8 @@ PYBIND11_MODULE(_native, m) {
           py::arg("negative_sample_rate") = 5.0f, py::arg("loss") = 0, py::arg("mid_rate") = 0.25f,
           py::arg("walk_len") = 4, py::arg("n_fixed") = 0, py::arg("mid_pairs") = py::none(),
           py::arg("indptr") = py::none(), py::arg("indices") = py::none(), py::arg("seed") = 0,
-          py::arg("stream_mode") = 0);
+          py::arg("stream_mode") = 0, py::arg("walk_lens") = py::none(), py::arg("jump_indptr") = py::none(),
+          py::arg("jump_indices") = py::none(), py::arg("mid_jump") = 0.0f);
     m.def("tsne_attraction", [](py::object indptr, py::object indices, py::object data, py::object Y, float dof, int) {
               auto ip = view<int32_t>(indptr), ix = view<int32_t>(indices);
               auto P = view<float>(data);

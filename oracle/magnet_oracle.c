@@ -11,6 +11,8 @@
  *   orc_rng_*           src/rng.hpp:5-28            (splitmix64 seeding, xorshift64*, below, uniform)
  *   orc_sgd_serial      src/layout.cpp:90-116 (apply_step), :118-276 (epoch_worker, hogwild path),
  *                       :281-297 (run_epochs, single-thread path), :343-472 (optimize_layout argument rules)
+ *   orc_sgd_owner       src/layout.cpp:118-276 (epoch_worker, OWNER = true), :300-330 (owner epochs), :441-463
+ *                       (chunks at the edge quantiles), :31-40 (the owner attraction scale 1.5)
  *   orc_sgd_schedule    the draws epoch_worker makes (src/layout.cpp:123,135,160-166,184,226-249), recorded
  *                       instead of applied; one stream per epoch (tid 0, the n_threads=1 reference), or the
  *                       device fast mode's counter draws (each draw of a sample addressed by edge and index)
@@ -345,6 +347,163 @@ int64_t orc_sgd_schedule(orc_sgd_args* c, int epoch, int per_edge_stream,
     orc_record rec = {sampled, n_neg, neg_off, negs, negs_cap, mid, 0};
     orc_epoch(c, &dv, epoch, alpha, mid_w, per_edge_stream, 0, &rec);
     return rec.n_negs;
+}
+
+/* Owner mode (parallel = 1; src/layout.cpp:118-276 with OWNER = true, :300-330, :441-463), UMAP loss only.
+ * Nodes are split at the edge quantiles into n_chunks = min(4096, max(1, E / 4096)) chunks (edges sorted by head);
+ * chunk k of epoch e draws from its own stream (tid = k) over its edges in order, moves only its own heads u
+ * (the attraction scaled by 1.5), and reads every other position from the layout as it was at the start of the
+ * epoch. The reference's two alternating snapshot buffers hold exactly that layout, so one copy per epoch
+ * restates them. With the reverse mid pairs (rev_indptr / rev_indices), u also receives, after each edge, the
+ * mid-range pulls of the nodes that chose it. The result does not depend on the order the chunks run in. */
+static void orc_owner_chunk(orc_sgd_args* c, const orc_derived* dv, int epoch, float alpha, float mid_w, int k,
+                            int64_t e0, int64_t e1, const float* Yr, const int32_t* rev_indptr,
+                            const int32_t* rev_indices) {
+    const int dim = c->dim;
+    orc_rng rng; orc_rng_seed(&rng, orc_stream_seed(c->seed, epoch, (uint64_t)k));
+    /* n_mid stays set when a jump graph replaces the pairs (src/layout.cpp:397-407) */
+    const float inv_n_mid = c->n_mid > 0 ? 1.0f / (float)c->n_mid : 0.0f;
+    const float pair_scale = 1.5f;
+    const float fepoch = (float)epoch;
+    float diff[ORC_MAX_DIM], gu[ORC_MAX_DIM], gk[ORC_MAX_DIM];
+    for (int64_t i = e0; i < e1; ++i) {
+        if (c->eons[i] > fepoch) continue;
+        const int32_t u = c->head[i], v = c->tail[i];
+        float* yu = c->Y + (int64_t)u * dim;
+        const float* yv = Yr + (int64_t)v * dim;
+        const int move_u = u >= c->n_fixed;
+        for (int q = 0; q < dim; ++q) gu[q] = 0.0f;
+        float d2 = 0.0f;
+        for (int q = 0; q < dim; ++q) { diff[q] = yu[q] - yv[q]; d2 += diff[q] * diff[q]; }
+        const float b_u = c->node_b ? c->node_b[u] : c->b;
+        const float b_uv = c->node_b ? 0.5f * (c->node_b[u] + c->node_b[v]) : c->b;
+        const float pw_v = (dv->b_is_one && !c->node_b) ? d2 : (d2 > 0.0f ? powf(d2, b_uv) : 0.0f);
+        if (d2 > 0.0f) {
+            float coeff;
+            if (c->kernel == 0) coeff = -pair_scale * c->exaggeration * 2.0f * c->a * b_uv * pw_v / (d2 * (c->a * pw_v + 1.0f));
+            else if (c->kernel == 1) coeff = -pair_scale * c->exaggeration * 2.0f * c->a;
+            else if (c->kernel == 2) { const float dd = sqrtf(d2); coeff = -pair_scale * c->exaggeration * c->a * tanhf(c->a * dd) / dd; }
+            else coeff = -pair_scale * c->exaggeration * 2.0f * c->a * (1.0f + tanhf(c->a * d2));
+            for (int q = 0; q < dim; ++q) gu[q] += coeff * diff[q];
+        }
+        c->eons[i] += c->eps[i];
+        const float epn = c->eps[i] / c->negative_sample_rate;
+        const int n_neg = (int)((fepoch - c->eonns[i]) / epn);
+        for (int p = 0; p < n_neg; ++p) {
+            const int32_t kk = (int32_t)orc_rng_below(&rng, (uint32_t)c->n);
+            if (kk == u) continue;
+            const float* yk = Yr + (int64_t)kk * dim;
+            float dd = 0.0f;
+            for (int q = 0; q < dim; ++q) { diff[q] = yu[q] - yk[q]; dd += diff[q] * diff[q]; }
+            if (dd > 0.0f) {
+                float coeff;
+                if (c->kernel == 0) {
+                    if (c->node_b && dv->rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c->repulsion_strength / ((0.001f + dd) * (c->a * pw + 1.0f)); }
+                    else { const float pw = dv->rep_b_is_one ? dd : powf(dd, c->rep_b); coeff = dv->two_b / ((0.001f + dd) * (c->rep_a * pw + 1.0f)); }
+                } else if (c->kernel == 1) {
+                    const float qq = expf(-c->a * dd);
+                    coeff = c->repulsion_strength * 2.0f * c->a * qq / fmaxf(1.0f - qq, 1e-3f);
+                } else if (c->kernel == 2) {
+                    const float r = sqrtf(dd); const float qq = 1.0f / coshf(c->a * r);
+                    coeff = c->repulsion_strength * c->a * qq * tanhf(c->a * r) / (r * fmaxf(1.0f - qq, 1e-3f));
+                } else {
+                    const float th = fmaxf(tanhf(c->a * dd), 1e-3f);
+                    coeff = c->repulsion_strength * 2.0f * c->a * (1.0f - th * th) / th;
+                }
+                for (int q = 0; q < dim; ++q) gu[q] += coeff * diff[q];
+            } else {
+                for (int q = 0; q < dim; ++q) gu[q] += (orc_rng_uniform(&rng) - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
+            }
+        }
+        c->eonns[i] += (float)n_neg * epn;
+        if (mid_w > 0.0f && orc_rng_uniform(&rng) < c->mid_rate) {
+            int32_t w = v;
+            if (c->jump_indptr && c->mid_jump > 0.0f) {
+                const int L = c->walk_lens ? c->walk_lens[v] : c->walk_len;
+                for (int h = 0; h < L; ++h) {
+                    const int32_t js = c->jump_indptr[w], je = c->jump_indptr[w + 1];
+                    if (je > js && orc_rng_uniform(&rng) < c->mid_jump) {
+                        w = c->jump_indices[js + (int32_t)orc_rng_below(&rng, (uint32_t)(je - js))];
+                    } else {
+                        const int32_t s0 = c->indptr[w], ee = c->indptr[w + 1];
+                        if (ee <= s0) break;
+                        w = c->indices[s0 + (int32_t)orc_rng_below(&rng, (uint32_t)(ee - s0))];
+                    }
+                }
+            } else if (c->mid_pairs) {
+                w = c->mid_pairs[(int64_t)u * c->n_mid + orc_rng_below(&rng, (uint32_t)c->n_mid)];
+            } else {
+                const int L = c->walk_lens ? c->walk_lens[v] : c->walk_len;
+                for (int h = 0; h < L; ++h) {
+                    const int32_t s0 = c->indptr[w], ee = c->indptr[w + 1];
+                    if (ee <= s0) break;
+                    w = c->indices[s0 + (int32_t)orc_rng_below(&rng, (uint32_t)(ee - s0))];
+                }
+            }
+            if (w != u) {
+                const float* yw = Yr + (int64_t)w * dim;
+                for (int q = 0; q < dim; ++q) gu[q] += -mid_w * (yu[q] - yw[q]);
+            }
+        }
+        if (move_u) orc_apply_step(c, yu, gu, alpha, u);
+        if (move_u && mid_w > 0.0f && rev_indptr) {
+            const int32_t rs = rev_indptr[u], re = rev_indptr[u + 1];
+            float p = c->mid_rate * (float)(re - rs) * inv_n_mid;
+            while (p > 0.0f && re > rs) {
+                if (orc_rng_uniform(&rng) < p) {
+                    const int32_t x = rev_indices[rs + (int32_t)orc_rng_below(&rng, (uint32_t)(re - rs))];
+                    if (x != u) {
+                        const float* yx = Yr + (int64_t)x * dim;
+                        for (int q = 0; q < dim; ++q) gk[q] = -mid_w * (yu[q] - yx[q]);
+                        orc_apply_step(c, yu, gk, alpha, u);
+                    }
+                }
+                p -= 1.0f;
+            }
+        }
+    }
+}
+
+/* chunk boundaries of owner mode (src/layout.cpp:441-463): own[k] the first node, eown[k] the first edge of chunk
+ * k; both arrays hold n_chunks + 1 entries. Returns n_chunks (own / eown NULL: only the count). */
+int orc_owner_chunks(const int32_t* head, int64_t n_edges, int64_t n, int64_t* own, int64_t* eown) {
+    int64_t nc = n_edges / 4096;
+    if (nc < 1) nc = 1;
+    if (nc > 4096) nc = 4096;
+    if (!own || !eown) return (int)nc;
+    for (int64_t t = 0; t <= nc; ++t) { own[t] = 0; eown[t] = 0; }
+    own[nc] = n; eown[nc] = n_edges;
+    for (int64_t t = 1; t < nc; ++t) {
+        const int64_t e = n_edges * t / nc;
+        int64_t node = head[e] > own[t - 1] ? head[e] : own[t - 1];
+        own[t] = node;
+        int64_t k = eown[t - 1];
+        while (k < n_edges && head[k] < node) ++k;
+        eown[t] = k;
+    }
+    return (int)nc;
+}
+
+/* optimize_layout with parallel = 1 (owner mode); rev_indptr / rev_indices may be NULL. Returns 0, or -1 when the
+ * edges are not sorted by head or the loss is InfoNCE (the reference's argument errors). */
+int orc_sgd_owner(orc_sgd_args* c, const int32_t* rev_indptr, const int32_t* rev_indices) {
+    if (c->loss != 0) return -1;
+    for (int64_t i = 1; i < c->n_edges; ++i) if (c->head[i - 1] > c->head[i]) return -1;
+    orc_derived dv; orc_derive(c, &dv);
+    const int nc = orc_owner_chunks(c->head, c->n_edges, c->n, NULL, NULL);
+    int64_t* own = (int64_t*)malloc(sizeof(int64_t) * (nc + 1));
+    int64_t* eown = (int64_t*)malloc(sizeof(int64_t) * (nc + 1));
+    orc_owner_chunks(c->head, c->n_edges, c->n, own, eown);
+    const size_t bytes = sizeof(float) * (size_t)c->n * (size_t)c->dim;
+    float* Yr = (float*)malloc(bytes > 0 ? bytes : 1);
+    for (int e = c->epoch_start; e < c->epoch_end; ++e) {
+        float alpha, mid_w; orc_sched(c, &dv, e, &alpha, &mid_w);
+        memcpy(Yr, c->Y, bytes);
+        for (int k = 0; k < nc; ++k)
+            orc_owner_chunk(c, &dv, e, alpha, mid_w, k, eown[k], eown[k + 1], Yr, rev_indptr, rev_indices);
+    }
+    free(Yr); free(own); free(eown);
+    return 0;
 }
 
 /* ------------------------------------------------------------------ FFT repulsion pieces (src/fftconv.cpp) */

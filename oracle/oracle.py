@@ -80,6 +80,10 @@ def lib():
         L.orc_rng_stream.argtypes = [ctypes.c_uint64, _I64, _P]
         L.orc_sgd_serial.argtypes = [ctypes.POINTER(SgdArgs), ctypes.c_int]
         L.orc_sgd_serial.restype = ctypes.c_int
+        L.orc_sgd_owner.argtypes = [ctypes.POINTER(SgdArgs), _P, _P]
+        L.orc_sgd_owner.restype = ctypes.c_int
+        L.orc_owner_chunks.argtypes = [_P, _I64, _I64, _P, _P]
+        L.orc_owner_chunks.restype = ctypes.c_int
         L.orc_sgd_schedule.argtypes = [ctypes.POINTER(SgdArgs), ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _I64, _P]
         L.orc_sgd_schedule.restype = _I64
         L.orc_spread.argtypes = [_P, _I64, _F, _F, _F, ctypes.c_int, ctypes.c_int, _P]
@@ -171,6 +175,26 @@ def sgd_serial(Y, head, tail, eps, eons, eonns, per_edge_stream=False, **kw):
         assert a.flags.c_contiguous
     args = _sgd_args(Y, head, tail, eps, eons, eonns, **kw)
     lib().orc_sgd_serial(ctypes.byref(args), int(bool(per_edge_stream)))
+
+
+def sgd_owner(Y, head, tail, eps, eons, eonns, rev_indptr=None, rev_indices=None, **kw):
+    """optimize_layout with parallel=1 (owner mode), in place; the result does not depend on the thread count."""
+    for a in (Y, eons, eonns):
+        assert a.flags.c_contiguous
+    args = _sgd_args(Y, head, tail, eps, eons, eonns, **kw)
+    rp = None if rev_indptr is None or rev_indptr.size == 0 else _c32(rev_indptr, np.int32)
+    rx = None if rp is None else _c32(rev_indices, np.int32)
+    if lib().orc_sgd_owner(ctypes.byref(args), _ptr(rp), _ptr(rx)) != 0:
+        raise ValueError("owner mode needs edges sorted by head and the umap loss")
+
+
+def owner_chunks(head, n):
+    """(own, eown): first node and first edge of each owner-mode chunk, n_chunks + 1 entries each"""
+    head = _c32(head, np.int32)
+    nc = lib().orc_owner_chunks(head.ctypes.data, head.shape[0], n, None, None)
+    own = np.zeros(nc + 1, np.int64); eown = np.zeros(nc + 1, np.int64)
+    lib().orc_owner_chunks(head.ctypes.data, head.shape[0], n, own.ctypes.data, eown.ctypes.data)
+    return own, eown
 
 
 def sgd_schedule(Y, head, tail, eps, eons, eonns, epoch, per_edge_stream=False, negs_cap=None, **kw):

@@ -6,11 +6,11 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for p in (ROOT, os.path.join(ROOT, "lib-magnet_b200")):
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+# GOLDEN holds sgd_cases.py, the option cases shared by the fixture script and the tests
+for p in (ROOT, os.path.join(ROOT, "lib-magnet_b200"), GOLDEN):
     if p not in sys.path:
         sys.path.insert(0, p)
-
-GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def pytest_configure(config):

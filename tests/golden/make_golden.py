@@ -6,7 +6,7 @@ by the reference's own code: its compiled `_magnet` (optimize_layout at n_thread
 tsne_step, bbox_2d) and its Python drivers (magnet/tsne.py FFTRepulsion2D / optimize_tsne, magnet/knn.py
 fuzzy_graph, magnet/__init__.py edge schedule). Inputs are seeded synthetic data.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner]
 """
 import os
 import sys
@@ -19,6 +19,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.environ.get("MAGNET_REFERENCE_DIR", "/root/reference")
 sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))   # the compiled reference module, importable as _magnet
 sys.path.insert(0, REF)
+sys.path.insert(0, HERE)
 
 import _magnet  # noqa: E402  (the reference's native module)
 from magnet import MAGNET  # noqa: E402
@@ -143,10 +144,63 @@ def tsne_fixture():
                         U=U, G=G, Fr=Fr, Ys=Ys, Us=Us, Gs=Gs, Y_tsne60=Yt)
 
 
+def sgd_options_fixture():
+    """the reference's optimize_layout (n_threads=1) on each option case of sgd_cases.py: the final Y, eons, eonns
+    and Adam state at seed 12345, and the 10-NN label purity of its layouts at seeds 1..8 (sgd_cases.expected reads
+    them back)"""
+    import sgd_cases
+    g = dict(np.load(os.path.join(HERE, "sgd_small.npz")))
+    out = {}
+    for name in sgd_cases.CASES:
+        Y, eons, eonns, kw = sgd_cases.state(g, name)
+        _magnet.optimize_layout(Y, g["head"], g["tail"], g["eps"], eons, eonns, n_threads=1, **kw)
+        out[f"Y_{name}"] = Y
+        # the bookkeeping is stored only where it differs from the default run's (sgd_small.npz eons_default)
+        if not np.array_equal(eons, g["eons_default"]):
+            out[f"eons_{name}"] = eons
+        if not np.array_equal(eonns, g["eonns_default"]):
+            out[f"eonns_{name}"] = eonns
+        if kw["optimizer"] == 1:
+            out[f"adam_m_{name}"], out[f"adam_v_{name}"], out[f"adam_t_{name}"] = kw["adam_m"], kw["adam_v"], kw["adam_t"]
+        pur = []
+        for sd in range(1, 9):
+            Y, eons, eonns, kw = sgd_cases.state(g, name, seed=sd)
+            _magnet.optimize_layout(Y, g["head"], g["tail"], g["eps"], eons, eonns, n_threads=1, **kw)
+            pur.append(sgd_cases.purity(Y, g["labels"]))
+        out[f"purity_{name}"] = np.array(pur)
+    np.savez_compressed(os.path.join(HERE, "sgd_options.npz"), **out)
+
+
+def sgd_owner_fixture():
+    """the reference's owner mode (parallel=1, 4 threads; its result does not depend on the thread count) on each
+    owner case of sgd_cases.py: the final Y and sha-256 digests of eons, eonns and the Adam state at seed 12345,
+    and the 10-NN label purity of its layouts at seeds 1..8"""
+    import sgd_cases
+    g = dict(np.load(os.path.join(HERE, "sgd_small.npz")))
+    big = sgd_cases.synthetic_graph()
+    out = {}
+    for name in sgd_cases.OWNER_CASES:
+        for sd in [12345] + list(range(1, 9)):
+            gg, Y, eons, eonns, kw, rp, rx = sgd_cases.owner_state(g, name, seed=sd, big=big)
+            _magnet.optimize_layout(Y, gg["head"], gg["tail"], gg["eps"], eons, eonns, n_threads=4, parallel=1,
+                                    rev_indptr=rp, rev_indices=rx, **kw)
+            if sd == 12345:
+                out[f"Y_{name}"] = Y
+                keys = ["eons", "eonns"] + (["adam_m", "adam_v", "adam_t"] if kw["optimizer"] == 1 else [])
+                arrays = dict(eons=eons, eonns=eonns, **{k: kw[k] for k in keys[2:]})
+                out[f"digests_{name}"] = np.array([f"{k}:{sgd_cases.digest(arrays[k])}" for k in keys])
+            else:
+                out.setdefault(f"purity_{name}", []).append(sgd_cases.purity(Y, gg["labels"]))
+        out[f"purity_{name}"] = np.array(out[f"purity_{name}"])
+    np.savez_compressed(os.path.join(HERE, "sgd_owner.npz"), **out)
+
+
 if __name__ == "__main__":
-    sgd_fixture()
-    fft_fixture()
-    tsne_fixture()
+    # all fixtures, or only those named on the command line (sgd_options reads sgd_small.npz)
+    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner"]
+    for name in todo:
+        {"sgd": sgd_fixture, "fft": fft_fixture, "tsne": tsne_fixture, "sgd_options": sgd_options_fixture,
+         "sgd_owner": sgd_owner_fixture}[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

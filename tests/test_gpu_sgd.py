@@ -5,6 +5,7 @@ eons / eonns bookkeeping after a whole run equals the reference's bit-for-bit; l
 import numpy as np
 import pytest
 
+import sgd_cases as C
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -54,10 +55,7 @@ def run_layout(mg, g, stream_mode, case="default", seed=12345):
     return Y, eons, eonns
 
 
-def purity(Y, labels, k=10):
-    from sklearn.neighbors import NearestNeighbors
-    nn = NearestNeighbors(n_neighbors=k + 1).fit(Y).kneighbors(Y, return_distance=False)[:, 1:]
-    return float((labels[nn] == labels[:, None]).mean())
+purity = C.purity
 
 
 @pytest.mark.parametrize("stream_mode", [0, 1])
@@ -109,3 +107,63 @@ def test_argument_errors(mg, golden):
                            1.0, 5.0, 3, 1.0, 2.0, 4, 0.25, 0, 0, 0, np.zeros((0, 2), np.float32),
                            np.zeros((0, 2), np.float32), z, 0.9, 0.999, z, np.zeros((0, 1), np.int32), z, z, 0.0, 0,
                            np.zeros(0, np.float32), 7, 1, 0)
+
+
+SCHEDULE_KEYS = ("epoch_start", "epoch_end", "alpha0", "alpha1", "mid_w0", "mid_w1", "negative_sample_rate", "loss",
+                 "mid_rate", "walk_len", "n_fixed", "mid_pairs", "indptr", "indices", "seed", "walk_lens",
+                 "jump_indptr", "jump_indices", "mid_jump")
+
+
+@pytest.mark.parametrize("stream_mode", [1, 0])
+@pytest.mark.parametrize("case", C.SCHEDULE_CASES)
+def test_option_schedule_bit_exact(mg, golden, stream_mode, case):
+    """InfoNCE negatives, jump-graph and per-node-length walks and a 3-d layout: the device's draws of six epochs
+    equal the oracle's (the reference's single stream in the serial mode, its per-edge replay in the counter mode)"""
+    g = golden("sgd_small.npz")
+    Y, e_o, en_o, kw = C.state(g, case)
+    _, e_d, en_d, _ = C.state(g, case)
+    for epoch in range(6):
+        rec_o = O.sgd_schedule(Y.copy(), g["head"], g["tail"], g["eps"], e_o, en_o, epoch,
+                               per_edge_stream=(stream_mode == 0), **C.oracle_kw(kw))
+        rec_d = mg.layout_schedule(Y.copy(), g["head"], g["tail"], g["eps"], e_d, en_d, epoch,
+                                   stream_mode=stream_mode, **{k: kw[k] for k in SCHEDULE_KEYS})
+        assert np.array_equal(rec_o[0].astype(bool), rec_d[0].astype(bool))
+        for a, b in zip(rec_o[1:], rec_d[1:]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(e_o, e_d) and np.array_equal(en_o, en_d)
+
+
+def run_case(mg, g, case, stream_mode, seed=12345):
+    Y, eons, eonns, kw = C.state(g, case, seed)
+    mg.optimize_layout(Y, g["head"], g["tail"], g["eps"], eons, eonns, n_threads=1, stream_mode=stream_mode, **kw)
+    return Y, eons, eonns, kw
+
+
+@pytest.mark.parametrize("stream_mode", [0, 1])
+@pytest.mark.parametrize("case", C.CASES)
+def test_option_layout_against_reference(mg, golden, stream_mode, case):
+    """each option case on the device: the eons / eonns bookkeeping equals the reference's bit for bit, fixed
+    nodes stay put, Adam's per-node step counts equal the oracle's replay of the same draws (counter mode), and the
+    layout's 10-NN label purity over seeds 1..8 matches the reference's own 8 runs"""
+    g, opts = golden("sgd_small.npz"), golden("sgd_options.npz")
+    Y0 = C.state(g, case)[0]
+    if stream_mode == 1 and C.state(g, case)[3]["optimizer"] == 1:
+        with pytest.raises(RuntimeError, match="supports the sgd optimizer only"):
+            run_case(mg, g, case, stream_mode)
+        return
+    Y, eons, eonns, kw = run_case(mg, g, case, stream_mode)
+    _, eons_r, eonns_r = C.expected(g, opts, case)
+    assert np.array_equal(eons, eons_r) and np.array_equal(eonns, eonns_r)
+    assert np.isfinite(Y).all()
+    nf = kw["n_fixed"]
+    assert np.array_equal(Y[:nf], Y0[:nf]) and not np.array_equal(Y[nf:], Y0[nf:])
+    if kw["optimizer"] == 1:
+        Yo, eo, eno, kwo = C.state(g, case)
+        O.sgd_serial(Yo, g["head"], g["tail"], g["eps"], eo, eno, per_edge_stream=True, **C.oracle_kw(kwo))
+        assert np.array_equal(kw["adam_t"], kwo["adam_t"])
+        assert np.isfinite(kw["adam_m"]).all() and (kw["adam_v"] >= 0).all()
+    # the reference's own spread over seeds sets the tolerance (InfoNCE and Adam layouts of 40 epochs vary by
+    # several points of purity from seed to seed): 8-seed means within max(0.03, 1.5 std)
+    p_ref = opts[f"purity_{case}"]
+    p = np.mean([purity(run_case(mg, g, case, stream_mode, seed=sd)[0], g["labels"]) for sd in range(1, 9)])
+    assert p > p_ref.mean() - max(0.03, 1.5 * p_ref.std()), (p, p_ref.mean())

@@ -3,6 +3,7 @@ produced (tests/golden/make_golden.py): bit-exact for the SGD at n_threads=1 and
 import numpy as np
 import pytest
 
+import sgd_cases as C
 from oracle import oracle as O
 
 
@@ -35,6 +36,65 @@ def test_sgd_serial_bit_exact(golden, case):
     O.sgd_serial(Y, g["head"], g["tail"], eps, eons, eonns, **kw)
     assert np.array_equal(Y, g[f"Y_{case}"])
     assert np.array_equal(eons, g[f"eons_{case}"]) and np.array_equal(eonns, g[f"eonns_{case}"])
+
+
+@pytest.mark.parametrize("case", C.CASES)
+def test_sgd_options_bit_exact(golden, ref, case):
+    """InfoNCE, the gaussian / sech / tanh kernels, Adam, the norm clip, jump-graph and per-node walks, per-node b,
+    the coupled repulsion kernel, exaggeration and dims 3 and 8: the oracle's serial run equals the reference's
+    (stored in sgd_options.npz) bit for bit, Adam state included; and the reference run live when it is built"""
+    g, opts = golden("sgd_small.npz"), golden("sgd_options.npz")
+    Y, eons, eonns, kw = C.state(g, case)
+    O.sgd_serial(Y, g["head"], g["tail"], g["eps"], eons, eonns, **C.oracle_kw(kw))
+    Yr, eons_r, eonns_r = C.expected(g, opts, case)
+    assert np.array_equal(Y, Yr)
+    assert np.array_equal(eons, eons_r) and np.array_equal(eonns, eonns_r)
+    if kw["optimizer"] == 1:
+        for k in ("adam_m", "adam_v", "adam_t"):
+            assert np.array_equal(kw[k], opts[f"{k}_{case}"])
+    # every case changes the layout against the default options
+    assert Y.shape != g["Y_default"].shape or not np.array_equal(Y, g["Y_default"])
+    if ref is not None:
+        Y2, eons2, eonns2, kw2 = C.state(g, case)
+        ref.optimize_layout(Y2, g["head"], g["tail"], g["eps"], eons2, eonns2, n_threads=1, **kw2)
+        assert np.array_equal(Y2, Y) and np.array_equal(eons2, eons) and np.array_equal(eonns2, eonns)
+
+
+@pytest.fixture(scope="module")
+def big_graph():
+    return C.synthetic_graph()
+
+
+@pytest.mark.parametrize("case", C.OWNER_CASES)
+def test_sgd_owner_bit_exact(golden, ref, big_graph, case):
+    """owner mode (parallel=1): the oracle equals the reference's run (sgd_owner.npz: Y, and sha-256 digests of
+    eons, eonns and the Adam state) bit for bit, over 2 and 23 chunks, with reverse mid pairs, walks, jumps, fixed
+    nodes, dims 2, 3 and 8 and distance-0 jitter draws; and the reference run live when it is built"""
+    g, own = golden("sgd_small.npz"), golden("sgd_owner.npz")
+    gg, Y, eons, eonns, kw, rp, rx = C.owner_state(g, case, big=big_graph)
+    O.sgd_owner(Y, gg["head"], gg["tail"], gg["eps"], eons, eonns, rev_indptr=rp, rev_indices=rx, **C.oracle_kw(kw))
+    assert np.array_equal(Y, own[f"Y_{case}"])
+    arrays = dict(eons=eons, eonns=eonns, adam_m=kw["adam_m"], adam_v=kw["adam_v"], adam_t=kw["adam_t"])
+    for entry in own[f"digests_{case}"]:
+        k, h = str(entry).split(":")
+        assert C.digest(arrays[k]) == h, k
+    if ref is not None:
+        _, Y2, eons2, eonns2, kw2, _, _ = C.owner_state(g, case, big=big_graph)
+        ref.optimize_layout(Y2, gg["head"], gg["tail"], gg["eps"], eons2, eonns2, n_threads=3, parallel=1,
+                            rev_indptr=rp, rev_indices=rx, **kw2)
+        assert np.array_equal(Y2, Y) and np.array_equal(eons2, eons) and np.array_equal(eonns2, eonns)
+
+
+def test_owner_chunks_follow_edge_quantiles(big_graph):
+    """chunk boundaries at the edge quantiles, moved to node boundaries (src/layout.cpp:441-463)"""
+    head = big_graph["head"]
+    own, eown = O.owner_chunks(head, big_graph["Y0"].shape[0])
+    E, nc = head.shape[0], own.shape[0] - 1
+    assert nc == min(4096, max(1, E // 4096)) == 23
+    assert own[0] == 0 and own[-1] == big_graph["Y0"].shape[0] and eown[0] == 0 and eown[-1] == E
+    for t in range(1, nc):
+        assert own[t] == max(head[E * t // nc], own[t - 1])
+        assert eown[t] == np.searchsorted(head, own[t], "left")
 
 
 def test_tsne_kernels_bit_exact(golden):
