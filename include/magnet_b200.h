@@ -155,10 +155,16 @@ typedef struct {
     const float* node_b;         /* (n) or NULL */
     uint64_t seed;
     int n_threads;               /* accepted for signature parity; the device decides its own parallelism */
-    int parallel;                /* 0 hogwild (reference), accepted values as the reference */
-    int stream_mode;             /* 0 = counter-based draws per (epoch, edge, index) (fast, default);
+    int parallel;                /* 0 hogwild; 1 owner (src/layout.cpp:441-463): edges sorted by head, umap loss;
+                                    one stream per chunk of about 4096 edges, reads from the epoch-start layout;
+                                    deterministic, and bit-exact against the reference for the power kernel
+                                    with b = rep_b = 1 under the sgd optimizer */
+    int stream_mode;             /* hogwild only. 0 = counter-based draws per (epoch, edge, index) (fast, default);
                                     1 = the reference's single stream per epoch replayed exactly (serial mode),
                                         updates from an epoch snapshot in fixed point: deterministic */
+    /* owner mode: who chose each node as a mid-range partner, CSR (n + 1, rev_nnz), or NULL
+       (rev_indptr / rev_indices of src/bindings.cpp:23) */
+    const int32_t* rev_indptr; const int32_t* rev_indices; int64_t rev_nnz;
 } mg_layout_args;
 
 /* Fills a with the reference's defaults for the scalars (pointers NULL). */

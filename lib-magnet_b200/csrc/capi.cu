@@ -462,10 +462,9 @@ SgdDev prepare_sgd(const mg_layout_args& A, cudaStream_t s) {
     require(A.loss == 0 || A.kernel == 0, "the InfoNCE loss supports the power kernel only");
     require(A.parallel == 0 || A.parallel == 1, "parallel must be 0 (hogwild) or 1 (owner)");
     require(A.parallel == 0 || A.loss == 0, "parallel='owner' supports the umap loss only (InfoNCE moves the negatives)");
-    if (A.parallel == 1) throw Error(MG_ERR_NOT_SUPPORTED, "parallel='owner' is not available on the device path");
     require(A.n_fixed >= 0 && A.n_fixed <= n, "n_fixed out of range");
     require(A.stream_mode == 0 || A.stream_mode == 1, "stream_mode must be 0 (per-edge streams) or 1 (serial stream)");
-    if (A.stream_mode == 1 && A.optimizer == 1)
+    if (A.parallel == 0 && A.stream_mode == 1 && A.optimizer == 1)
         throw Error(MG_ERR_NOT_SUPPORTED, "the serial stream mode supports the sgd optimizer only");
     if (A.head && !is_device_ptr(A.head)) {
         // the reference's per-edge checks (src/layout.cpp:385-388); the first failing edge names the message
@@ -501,6 +500,31 @@ SgdDev prepare_sgd(const mg_layout_args& A, cudaStream_t s) {
     require(rep_a > 0.0f, "repulsion kernel a must be positive");
     if (A.node_b && !is_device_ptr(A.node_b))
         for (int64_t i = 0; i < n; ++i) require(A.node_b[i] > 0.05f && A.node_b[i] <= 2.0f, "node_b out of range");
+    if (A.parallel == 1) {
+        // src/layout.cpp:441-446; heads in device memory are checked on the device before the run
+        if (A.head && !is_device_ptr(A.head)) {
+            const int32_t* hd = A.head;
+            require(E < 2 || all_of_range(E - 1, [&](int64_t i) { return hd[i] <= hd[i + 1]; }),
+                    "parallel='owner' needs edges sorted by head");
+        }
+        if (A.rev_indptr) validate_csr_host(A.rev_indptr, A.rev_indices, A.rev_nnz, n, -1, "reverse pairs");
+        if (A.rev_indptr && has_pairs && use_mid) {
+            // the reverse pulls of an edge take p = mid_rate * row length / n_mid rounds of p -= 1
+            // (src/layout.cpp:262-273); in float that loop stops shrinking p above 2^24, so the device run
+            // requires a bound that keeps it short (the reference's loop would not end there either)
+            std::vector<int32_t> ip_h;
+            const int32_t* ip = A.rev_indptr;
+            if (is_device_ptr(ip)) {
+                ip_h.resize(n + 1);
+                MGB_CUDA(cudaMemcpy(ip_h.data(), ip, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost));
+                ip = ip_h.data();
+            }
+            int64_t longest = 0;
+            for (int64_t i = 0; i < n; ++i) longest = std::max<int64_t>(longest, (int64_t)ip[i + 1] - ip[i]);
+            require(std::isfinite(A.mid_rate) && A.mid_rate * (float)longest / (float)A.n_mid <= 65536.0f,
+                    "reverse pairs: mid_rate * row length / n_mid must be at most 65536");
+        }
+    }
 
     SgdDev c{};
     c.n = n; c.dim = dim; c.n_edges = E;
@@ -561,9 +585,18 @@ extern "C" int mg_optimize_layout(const mg_layout_args* a) {
         cudaStream_t s = current_stream();
         SgdDev c = prepare_sgd(*a, s);
         if (!g_sgd_work) g_sgd_work.reset(new SgdWork());
-        if (c.n_edges > 0 && a->epoch_end > a->epoch_start)
+        if (a->parallel == 1) {
+            if (is_device_ptr(a->head))
+                require(owner_heads_sorted(c.head, c.n_edges, *g_sgd_work, s), "parallel='owner' needs edges sorted by head");
+            const int32_t* rp = a->rev_indptr ? in_dev(a->rev_indptr, c.n + 1, 21, s) : nullptr;
+            const int32_t* rx = a->rev_indptr ? in_dev(a->rev_indices, a->rev_nnz, 22, s) : nullptr;
+            if (c.n_edges > 0 && a->epoch_end > a->epoch_start)
+                owner_run(c, *g_sgd_work, rp, rx, a->epoch_start, a->epoch_end, a->alpha0, a->alpha1, a->mid_w0,
+                          a->mid_w1, s);
+        } else if (c.n_edges > 0 && a->epoch_end > a->epoch_start) {
             sgd_run(c, *g_sgd_work, a->stream_mode, a->epoch_start, a->epoch_end, a->alpha0, a->alpha1, a->mid_w0,
                     a->mid_w1, s);
+        }
         sgd_copy_back(*a, c, s);
         if (any_host({a->Y, a->epoch_of_next_sample, a->epoch_of_next_negative_sample, a->adam_m}))
             MGB_CUDA(cudaStreamSynchronize(s));
@@ -576,6 +609,7 @@ extern "C" int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* s
         require(a != nullptr, "args must not be NULL");
         require(sampled && n_neg && neg_off && mid && n_negs, "outputs must not be NULL");
         require(epoch >= a->epoch_start && epoch < std::max(a->epoch_end, a->epoch_start + 1), "epoch outside the call's range");
+        if (a->parallel == 1) throw Error(MG_ERR_NOT_SUPPORTED, "the schedule hook records the hogwild draws only");
         cudaStream_t s = current_stream();
         SgdDev c = prepare_sgd(*a, s);
         if (!g_sgd_work) g_sgd_work.reset(new SgdWork());

@@ -792,13 +792,6 @@ void record_launch(const SgdDev& c, int epoch, float alpha, float mid_w, const i
     record_kernel<D><<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(c, epoch, alpha, mid_w, cnt, st, per_edge, rec);
 }
 
-#define MGB_DIM_DISPATCH(dim, F, ...)                \
-    switch (dim) {                                   \
-        case 2: F<2>(__VA_ARGS__); break;            \
-        case 3: F<3>(__VA_ARGS__); break;            \
-        default: F<0>(__VA_ARGS__); break;           \
-    }
-
 // row pointers when the edges are sorted by head, else nullptr (edge-parallel kernels)
 const int64_t* row_pointers(const SgdDev& c, SgdWork& w, cudaStream_t s) {
     if (c.n_edges == 0) return nullptr;

@@ -22,10 +22,20 @@ struct SgdDev {
     uint64_t seed;
 };
 
-// device scratch of the serial stream mode
+// launches F<2>, F<3> or the generic F<0> (dims up to kMaxDim) for a layout of `dim` columns
+#define MGB_DIM_DISPATCH(dim, F, ...)                \
+    switch (dim) {                                   \
+        case 2: F<2>(__VA_ARGS__); break;            \
+        case 3: F<3>(__VA_ARGS__); break;            \
+        default: F<0>(__VA_ARGS__); break;           \
+    }
+
+// device scratch of the stream modes and of owner mode
 struct SgdWork {
     DevBuf cnt, state, delta, eptr, flag;
     DevBuf samp;               // the epoch's per-edge negatives counts (counter mode fast path)
+    // owner mode: node rows, chunk bounds, per-edge negatives, per-node stream states, marked chunks, snapshots
+    DevBuf o_row, o_own, o_neg, o_state, o_dirty, o_snap, o_snap_m, o_snap_v, o_snap_t;
 };
 
 void sgd_sched(const SgdDev& c, int epoch, int e0, int e1, float alpha0, float alpha1, float mid_w0, float mid_w1,
@@ -37,5 +47,12 @@ void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha
 void sgd_record(SgdDev& c, SgdWork& w, int stream_mode, int epoch, float alpha, float mid_w, int32_t* n_neg_out,
                 int64_t* off_out, int32_t* negs, int64_t negs_cap, int32_t* mid, int64_t* n_negs_dev,
                 cudaStream_t s);
+
+// owner mode (parallel = 1, src/layout.cpp:441-463): chunk count for E edges, the sorted-heads check (device
+// heads; synchronises s), and epochs [e0, e1); the reverse mid pairs are device arrays or NULL
+int owner_chunk_count(int64_t n_edges);
+bool owner_heads_sorted(const int32_t* head_dev, int64_t n_edges, SgdWork& w, cudaStream_t s);
+void owner_run(SgdDev& c, SgdWork& w, const int32_t* rev_indptr, const int32_t* rev_indices, int e0, int e1,
+               float alpha0, float alpha1, float mid_w0, float mid_w1, cudaStream_t s);
 
 }  // namespace mgb

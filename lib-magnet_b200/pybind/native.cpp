@@ -162,7 +162,8 @@ void optimize_layout(py::object Y, py::object head, py::object tail, py::object 
     if (nb.size() > 0 && (nb.ndim() != 1 || nb.dim(0) != n)) throw std::runtime_error("node_b must have n entries");
     if (ip.size() > 0 && ip.size() != n + 1) throw std::runtime_error("indptr must have n + 1 entries");
     if (jp.size() > 0 && jp.size() != n + 1) throw std::runtime_error("indptr must have n + 1 entries");
-    (void)rev_indptr; (void)rev_indices;
+    auto rp = view<int32_t>(rev_indptr), rx = view<int32_t>(rev_indices);
+    if (rp.size() > 0 && rp.size() != n + 1) throw std::runtime_error("indptr must have n + 1 entries");
     mg_layout_args A;
     mg_layout_args_default(&A);
     A.Y = y.ptr; A.n = n; A.dim = dim;
@@ -182,6 +183,9 @@ void optimize_layout(py::object Y, py::object head, py::object tail, py::object 
     A.jump_nnz = jx.size(); A.mid_jump = mid_jump;
     A.kernel = kernel; A.node_b = nb.size() > 0 ? nb.ptr : nullptr; A.seed = seed; A.n_threads = n_threads;
     A.parallel = parallel; A.stream_mode = stream_mode;
+    if (parallel == 1 && rp.size() > 0) {
+        A.rev_indptr = rp.ptr; A.rev_indices = rx.size() > 0 ? rx.ptr : nullptr; A.rev_nnz = rx.size();
+    }
     py::gil_scoped_release rel;
     check(mg_optimize_layout(&A));
 }
