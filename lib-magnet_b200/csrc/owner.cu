@@ -9,10 +9,10 @@
 //
 // On the device one epoch is four steps on the caller's stream:
 //  1. snapshot: the layout (and the Adam state) is copied aside; it is the "start of the epoch" every read uses;
-//  2. chain pass, one thread per chunk: walks the chunk's edges in order, computes each sampled edge's negative
-//     count from eonns and advances eons / eonns as the reference does, and consumes the chunk's stream as the
-//     edge loop would (n_neg draws, the mid-range test and walk, the reverse-pull draws), recording at each head
-//     node the stream state where its edges start. It reads no position: the draws depend on positions only
+//  2. schedule, one thread per edge: advances eons / eonns as the reference does and records each sampled edge's
+//     negatives count; then the chain pass, one warp per chunk: consumes the chunk's stream in edge order as
+//     the edge loop would (n_neg draws, the mid-range test and walk, the reverse-pull draws), recording at each
+//     head node the stream state where its edges start. It reads no position: the draws depend on positions only
 //     through a negative at distance 0 exactly (src/layout.cpp:181), which draws dim extra uniforms;
 //  3. node pass, one thread per head node: from its recorded state, replays the node's edges as the reference
 //     does (other positions from the snapshot, its own in registers) and writes its row. A negative at distance 0
@@ -130,88 +130,97 @@ __device__ uint64_t owner_node(const SgdDev& c, const OwnerDev& o, int64_t u, ui
 #pragma unroll
     for (int d = 0; d < DM; ++d)
         if (d < dim) yu[d] = o.Yr[u * dim + d];
-    for (int64_t i = o.row[u]; i < o.row[u + 1]; ++i) {
-        const int n_neg = o.n_neg[i];
-        if (n_neg == kNotSampled) continue;
-        const int32_t v = c.tail[i];
-        const float* yv = o.Yr + (int64_t)v * dim;
-        float d2 = 0.0f;
-#pragma unroll
-        for (int d = 0; d < DM; ++d)
-            if (d < dim) { gu[d] = 0.0f; diff[d] = yu[d] - yv[d]; d2 += diff[d] * diff[d]; }
-        const float b_u = c.node_b ? c.node_b[u] : c.b;
-        const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
-        const float pw_v = (c.b_is_one && !c.node_b) ? d2 : (d2 > 0.0f ? powf(d2, b_uv) : 0.0f);
-        // attraction along the edge, the head only, scaled by 1.5
-        if (d2 > 0.0f) {
-            float coeff;
-            if (c.kernel == 0) coeff = -kOwnerAttraction * c.exaggeration * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
-            else if (c.kernel == 1) coeff = -kOwnerAttraction * c.exaggeration * 2.0f * c.a;
-            else if (c.kernel == 2) { const float dd = sqrtf(d2); coeff = -kOwnerAttraction * c.exaggeration * c.a * tanhf(c.a * dd) / dd; }
-            else coeff = -kOwnerAttraction * c.exaggeration * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
+    const int64_t row1 = o.row[u + 1];
+    for (int64_t w0 = o.row[u]; w0 < row1; w0 += 64) {
+        // the sampled edges of a window of 64 as a bit mask, taken in edge order
+        const int cnt = (int)(row1 - w0 < 64 ? row1 - w0 : 64);
+        uint64_t mask = 0;
+        for (int t = 0; t < cnt; ++t)
+            if (o.n_neg[w0 + t] != kNotSampled) mask |= 1ull << t;
+        while (mask) {
+            const int64_t i = w0 + (__ffsll((long long)mask) - 1);
+            mask &= mask - 1;
+            const int n_neg = o.n_neg[i];
+            const int32_t v = c.tail[i];
+            const float* yv = o.Yr + (int64_t)v * dim;
+            float d2 = 0.0f;
 #pragma unroll
             for (int d = 0; d < DM; ++d)
-                if (d < dim) gu[d] += coeff * diff[d];
-        }
-        // repulsion from the negatives, read from the snapshot
-        for (int p = 0; p < n_neg; ++p) {
-            const int32_t k = (int32_t)r.below((uint32_t)c.n);
-            if (k == u) continue;
-            const float* yk = o.Yr + (int64_t)k * dim;
-            float dd = 0.0f;
-#pragma unroll
-            for (int d = 0; d < DM; ++d)
-                if (d < dim) { diff[d] = yu[d] - yk[d]; dd += diff[d] * diff[d]; }
-            if (dd > 0.0f) {
+                if (d < dim) { gu[d] = 0.0f; diff[d] = yu[d] - yv[d]; d2 += diff[d] * diff[d]; }
+            const float b_u = c.node_b ? c.node_b[u] : c.b;
+            const float b_uv = c.node_b ? 0.5f * (c.node_b[u] + c.node_b[v]) : c.b;
+            const float pw_v = (c.b_is_one && !c.node_b) ? d2 : (d2 > 0.0f ? powf(d2, b_uv) : 0.0f);
+            // attraction along the edge, the head only, scaled by 1.5
+            if (d2 > 0.0f) {
                 float coeff;
-                if (c.kernel == 0) {
-                    if (c.node_b && c.rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f)); }
-                    else { const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b); coeff = c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f)); }
-                } else if (c.kernel == 1) {
-                    const float q = expf(-c.a * dd);
-                    coeff = c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
-                } else if (c.kernel == 2) {
-                    const float rr = sqrtf(dd); const float q = 1.0f / coshf(c.a * rr);
-                    coeff = c.repulsion_strength * c.a * q * tanhf(c.a * rr) / (rr * fmaxf(1.0f - q, 1e-3f));
-                } else {
-                    const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
-                    coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
-                }
+                if (c.kernel == 0) coeff = -kOwnerAttraction * c.exaggeration * 2.0f * c.a * b_uv * pw_v / (d2 * (c.a * pw_v + 1.0f));
+                else if (c.kernel == 1) coeff = -kOwnerAttraction * c.exaggeration * 2.0f * c.a;
+                else if (c.kernel == 2) { const float dd = sqrtf(d2); coeff = -kOwnerAttraction * c.exaggeration * c.a * tanhf(c.a * dd) / dd; }
+                else coeff = -kOwnerAttraction * c.exaggeration * 2.0f * c.a * (1.0f + tanhf(c.a * d2));
 #pragma unroll
                 for (int d = 0; d < DM; ++d)
                     if (d < dim) gu[d] += coeff * diff[d];
-            } else {
-                jitter = true;
-                for (int d = 0; d < dim; ++d) gu[d] += (r.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
             }
-        }
-        // mid-range partner, read from the snapshot
-        if (mid_w > 0.0f && r.uniform() < c.mid_rate) {
-            const int32_t w = mid_partner(c, r, u, v);
-            if (w != u) {
-                const float* yw = o.Yr + (int64_t)w * dim;
+            // repulsion from the negatives, read from the snapshot
+            for (int p = 0; p < n_neg; ++p) {
+                const int32_t k = (int32_t)r.below((uint32_t)c.n);
+                if (k == u) continue;
+                const float* yk = o.Yr + (int64_t)k * dim;
+                float dd = 0.0f;
 #pragma unroll
                 for (int d = 0; d < DM; ++d)
-                    if (d < dim) { const float g = -mid_w * (yu[d] - yw[d]); gu[d] += g; }
-            }
-        }
-        if (move_u) owner_step<DM>(c, yu, gu, alpha, u, dim);
-        // the pulls of the nodes that chose u as their partner, each its own step
-        if (move_u && mid_w > 0.0f && o.rev_indptr) {
-            const int32_t rs = o.rev_indptr[u], re = o.rev_indptr[u + 1];
-            float p = c.mid_rate * (float)(re - rs) * inv_n_mid;
-            while (p > 0.0f && re > rs) {
-                if (r.uniform() < p) {
-                    const int32_t x = o.rev_indices[rs + (int32_t)r.below((uint32_t)(re - rs))];
-                    if (x != u) {
-                        const float* yx = o.Yr + (int64_t)x * dim;
-#pragma unroll
-                        for (int d = 0; d < DM; ++d)
-                            if (d < dim) gk[d] = -mid_w * (yu[d] - yx[d]);
-                        owner_step<DM>(c, yu, gk, alpha, u, dim);
+                    if (d < dim) { diff[d] = yu[d] - yk[d]; dd += diff[d] * diff[d]; }
+                if (dd > 0.0f) {
+                    float coeff;
+                    if (c.kernel == 0) {
+                        if (c.node_b && c.rep_coupled) { const float pw = powf(dd, b_u); coeff = 2.0f * b_u * c.repulsion_strength / ((0.001f + dd) * (c.a * pw + 1.0f)); }
+                        else { const float pw = c.rep_b_is_one ? dd : powf(dd, c.rep_b); coeff = c.two_b / ((0.001f + dd) * (c.rep_a * pw + 1.0f)); }
+                    } else if (c.kernel == 1) {
+                        const float q = expf(-c.a * dd);
+                        coeff = c.repulsion_strength * 2.0f * c.a * q / fmaxf(1.0f - q, 1e-3f);
+                    } else if (c.kernel == 2) {
+                        const float rr = sqrtf(dd); const float q = 1.0f / coshf(c.a * rr);
+                        coeff = c.repulsion_strength * c.a * q * tanhf(c.a * rr) / (rr * fmaxf(1.0f - q, 1e-3f));
+                    } else {
+                        const float th = fmaxf(tanhf(c.a * dd), 1e-3f);
+                        coeff = c.repulsion_strength * 2.0f * c.a * (1.0f - th * th) / th;
                     }
+#pragma unroll
+                    for (int d = 0; d < DM; ++d)
+                        if (d < dim) gu[d] += coeff * diff[d];
+                } else {
+                    jitter = true;
+                    for (int d = 0; d < dim; ++d) gu[d] += (r.uniform() - 0.5f) * 1e-3f / fmaxf(alpha, 1e-6f);
                 }
-                p -= 1.0f;
+            }
+            // mid-range partner, read from the snapshot
+            if (mid_w > 0.0f && r.uniform() < c.mid_rate) {
+                const int32_t w = mid_partner(c, r, u, v);
+                if (w != u) {
+                    const float* yw = o.Yr + (int64_t)w * dim;
+#pragma unroll
+                    for (int d = 0; d < DM; ++d)
+                        if (d < dim) { const float g = -mid_w * (yu[d] - yw[d]); gu[d] += g; }
+                }
+            }
+            if (move_u) owner_step<DM>(c, yu, gu, alpha, u, dim);
+            // the pulls of the nodes that chose u as their partner, each its own step
+            if (move_u && mid_w > 0.0f && o.rev_indptr) {
+                const int32_t rs = o.rev_indptr[u], re = o.rev_indptr[u + 1];
+                float p = c.mid_rate * (float)(re - rs) * inv_n_mid;
+                while (p > 0.0f && re > rs) {
+                    if (r.uniform() < p) {
+                        const int32_t x = o.rev_indices[rs + (int32_t)r.below((uint32_t)(re - rs))];
+                        if (x != u) {
+                            const float* yx = o.Yr + (int64_t)x * dim;
+#pragma unroll
+                            for (int d = 0; d < DM; ++d)
+                                if (d < dim) gk[d] = -mid_w * (yu[d] - yx[d]);
+                            owner_step<DM>(c, yu, gk, alpha, u, dim);
+                        }
+                    }
+                    p -= 1.0f;
+                }
             }
         }
     }
@@ -254,31 +263,59 @@ __global__ void owner_sorted_kernel(const int32_t* __restrict__ head, int64_t E,
 }
 
 // ---------------------------------------------------------------------------------------------- epoch kernels
-__global__ void __launch_bounds__(32) owner_chain_kernel(SgdDev c, OwnerDev o, int epoch, float mid_w) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+// the epoch's schedule, one thread per edge (coalesced): eons / eonns advanced as src/layout.cpp:135,160-163,184
+// advance them, and each edge's negatives count recorded (kNotSampled when eons[i] > epoch)
+__global__ void __launch_bounds__(256) owner_schedule_kernel(SgdDev c, OwnerDev o, int epoch) {
+    const float fepoch = (float)epoch;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n_edges;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float eo = c.eons[i];
+        if (eo > fepoch) { o.n_neg[i] = kNotSampled; continue; }
+        const float ep = c.eps[i];
+        c.eons[i] = eo + ep;
+        const float epn = ep / c.negative_sample_rate;
+        const float en = c.eonns[i];
+        const int n_neg = (int)((fepoch - en) / epn);
+        c.eonns[i] = en + (float)n_neg * epn;
+        o.n_neg[i] = n_neg;
+    }
+}
+
+// One warp per chunk: the chunk's stream consumed in edge order from the recorded negatives counts. The lanes
+// read 32 edges' counts at a time (coalesced) and take the sampled ones in order from a ballot; every lane holds
+// the same stream state and makes the same draws, so control flow stays uniform across the warp. No position is
+// read and nothing is stored but the per-node states.
+constexpr int kChainWarps = 4;   // chunks per block
+
+__global__ void __launch_bounds__(32 * kChainWarps) owner_chain_kernel(SgdDev c, OwnerDev o, int epoch,
+                                                                        float mid_w) {
+    const int k = blockIdx.x * kChainWarps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (k >= o.n_chunks) return;
     Rng r(stream_seed(c.seed, epoch, (uint64_t)k));
-    const float fepoch = (float)epoch;
     const float inv_n_mid = c.n_mid > 0 ? 1.0f / (float)c.n_mid : 0.0f;
+    const int32_t* __restrict__ rec = o.n_neg;
     for (int64_t u = o.own[k]; u < o.own[k + 1]; ++u) {
-        o.node_state[u] = r.s;
-        const bool move_u = u >= c.n_fixed;
-        for (int64_t i = o.row[u]; i < o.row[u + 1]; ++i) {
-            if (c.eons[i] > fepoch) { o.n_neg[i] = kNotSampled; continue; }
-            c.eons[i] += c.eps[i];
-            const float epn = c.eps[i] / c.negative_sample_rate;
-            const int n_neg = (int)((fepoch - c.eonns[i]) / epn);
-            c.eonns[i] += (float)n_neg * epn;
-            o.n_neg[i] = n_neg;
-            for (int p = 0; p < n_neg; ++p) r.next();
-            if (mid_w > 0.0f && r.uniform() < c.mid_rate) (void)mid_partner(c, r, u, c.tail[i]);
-            if (move_u && mid_w > 0.0f && o.rev_indptr) {
-                const int32_t rs = o.rev_indptr[u], re = o.rev_indptr[u + 1];
-                float p = c.mid_rate * (float)(re - rs) * inv_n_mid;
-                while (p > 0.0f && re > rs) {
+        if (lane == 0) o.node_state[u] = r.s;
+        // the reverse-pull rounds of each of u's edges: the same p for every edge of u
+        float p0 = 0.0f;
+        if (u >= c.n_fixed && mid_w > 0.0f && o.rev_indptr) {
+            const int32_t rs = o.rev_indptr[u], re = o.rev_indptr[u + 1];
+            if (re > rs) p0 = c.mid_rate * (float)(re - rs) * inv_n_mid;
+        }
+        const int64_t i0 = o.row[u], i1 = o.row[u + 1];
+        for (int64_t base = i0; base < i1; base += 32) {
+            const int64_t i = base + lane;
+            const int mine = i < i1 ? __ldg(rec + i) : kNotSampled;
+            unsigned todo = __ballot_sync(0xffffffffu, mine != kNotSampled);
+            while (todo) {
+                const int b = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int n_neg = __shfl_sync(0xffffffffu, mine, b);
+                for (int p = 0; p < n_neg; ++p) r.next();
+                if (mid_w > 0.0f && r.uniform() < c.mid_rate) (void)mid_partner(c, r, u, c.tail[base + b]);
+                for (float p = p0; p > 0.0f; p -= 1.0f)
                     if (r.uniform() < p) (void)r.next();
-                    p -= 1.0f;
-                }
             }
         }
     }
@@ -382,7 +419,9 @@ void owner_run(SgdDev& c, SgdWork& w, const int32_t* rev_indptr, const int32_t* 
             MGB_CUDA(cudaMemcpyAsync(snap_v, c.adam_v, sizeof(float) * n * dim, cudaMemcpyDeviceToDevice, s));
             MGB_CUDA(cudaMemcpyAsync(snap_t, c.adam_t, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
         }
-        owner_chain_kernel<<<ceil_div(nc, 32), 32, 0, s>>>(c, o, epoch, mid_w);
+        owner_schedule_kernel<<<std::min(ceil_div(E, 256), 8 * kNumSMs), 256, 0, s>>>(c, o, epoch);
+        MGB_LAUNCH_CHECK();
+        owner_chain_kernel<<<ceil_div(nc, kChainWarps), 32 * kChainWarps, 0, s>>>(c, o, epoch, mid_w);
         MGB_LAUNCH_CHECK();
         MGB_DIM_DISPATCH(dim, owner_epoch_launch, c, o, epoch, alpha, mid_w, s);
     }

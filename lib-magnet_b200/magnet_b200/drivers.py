@@ -212,11 +212,22 @@ def optimize_sgd(Y, head, tail, epochs_per_sample, n_epochs, *, a, b, rep_a=None
                  mid_weight=0.0, mid_phase=0.5, mid_pairs=None, graph=None, walk_len=4, mid_rate=0.25,
                  negative_sample_rate=5.0, repulsion_strength=2.0, exaggeration=1.0, late_exaggeration=1.0,
                  late_phase=0.2, loss=0, kernel=0, optimizer=0, clip=0, n_fixed=0, seed=0, stream_mode=0,
-                 node_b=None, beta1=0.9, beta2=0.999):
+                 node_b=None, beta1=0.9, beta2=0.999, parallel="hogwild", jump_graph=None, mid_jump=0.5,
+                 walk_lens=None):
     """The sampled SGD pass of MAGNET._optimize (magnet/__init__.py:751-839, integer n_epochs): eons / eonns
     initialised from the schedule, linear learning-rate decay lr (1 - e / total), mid-range weight
     mid_weight max(0, 1 - e / (mid_phase total)), segments at the late-exaggeration boundary, each segment one
-    device optimize_layout call. Y is updated in place."""
+    device optimize_layout call. Y is updated in place.
+
+    parallel: "hogwild" (the device's draws per stream_mode), "serial" (the reference's single stream replayed
+    exactly, stream_mode 1) or "owner" (the reference's owner mode, magnet/__init__.py:758-761, 789-794: with
+    mid-near pairs and no jump graph, each node also receives the pulls of the nodes that chose it).
+    jump_graph: CSR of mid-range jumps taken with probability mid_jump on each walk step; walk_lens: per-node walk
+    lengths (magnet/__init__.py:774-786)."""
+    if parallel not in ("hogwild", "owner", "serial"):
+        raise ValueError("parallel must be 'hogwild', 'serial' or 'owner'")
+    if parallel == "owner" and loss == 1:
+        raise ValueError("parallel='owner' is not available with loss='infonce' (the negatives are moved)")
     n, dim = Y.shape
     total = int(n_epochs)
     lr = float(learning_rate)
@@ -238,6 +249,22 @@ def optimize_sgd(Y, head, tail, epochs_per_sample, n_epochs, *, a, b, rep_a=None
     else:
         am = av = np.zeros((0, dim), np.float32); at = z32
     nb = np.zeros(0, np.float32) if node_b is None else np.ascontiguousarray(node_b, dtype=np.float32)
+    if jump_graph is not None:
+        J = sp.csr_matrix(jump_graph)
+        jp, jx, mj = J.indptr.astype(np.int32), J.indices.astype(np.int32), float(mid_jump)
+    else:
+        jp, jx, mj = z32, z32, 0.0
+    wl = z32 if walk_lens is None or not use_mid else np.ascontiguousarray(walk_lens, dtype=np.int32)
+    rp = rx = z32
+    if parallel == "owner" and mid_pairs.size > 0 and jump_graph is None:
+        m = mid_pairs.shape[1]
+        R = sp.csr_matrix((np.ones(mid_pairs.size, np.float32), (mid_pairs.ravel(), np.repeat(np.arange(n), m))),
+                          shape=(n, n))
+        R.sort_indices()
+        rp, rx = R.indptr.astype(np.int32), R.indices.astype(np.int32)
+    par = 1 if parallel == "owner" else 0
+    if parallel == "serial":
+        stream_mode = 1
     mid_len = max(1.0, mid_phase * total)
     alpha = lambda e: lr * (1.0 - e / total)
     mid = (lambda e: mid_weight * max(0.0, 1.0 - e / mid_len)) if use_mid else (lambda e: 0.0)
@@ -251,8 +278,8 @@ def optimize_sgd(Y, head, tail, epochs_per_sample, n_epochs, *, a, b, rep_a=None
                           float(alpha(e0)), float(alpha(e1)), float(mid(e0)), float(mid(e1)), float(a), float(b),
                           float(rep_a), float(rep_b), float(negative_sample_rate), int(loss), float(exag),
                           float(repulsion_strength), int(walk_len), float(mid_rate), int(optimizer), int(clip),
-                          int(n_fixed), am, av, at, float(beta1), float(beta2), z32, mid_pairs, z32, z32, 0.0,
-                          int(kernel), nb, int(seed), -1, 0, None, None, int(stream_mode))
+                          int(n_fixed), am, av, at, float(beta1), float(beta2), wl, mid_pairs, jp, jx, mj,
+                          int(kernel), nb, int(seed), -1, par, rp, rx, int(stream_mode))
     return Y
 
 

@@ -88,3 +88,29 @@ def test_owner_argument_errors(mg, golden, big_graph):
         mg.optimize_layout(Y, gg["head"], gg["tail"], gg["eps"], eons, eonns, n_threads=1, parallel=1,
                            rev_indptr=rp, rev_indices=rx, **kw)
     assert np.array_equal(Y, C.owner_state(g, "b1_pairs", big=big_graph)[1])
+
+
+def test_owner_driver_on_blobs(mg):
+    """the reference's owner-mode test (tests/test_magnet.py:387-401) through the package's SGD driver: a 3000-point
+    6-blob kNN graph, 40 epochs with graph walks; two runs agree bit for bit and a 10-NN classifier on the layout
+    scores above 0.95; InfoNCE is refused"""
+    from sklearn.datasets import make_blobs
+    from sklearn.neighbors import KNeighborsClassifier, kneighbors_graph
+    from magnet_b200 import graph as G
+    X, y = make_blobs(n_samples=3000, centers=6, n_features=20, random_state=0)
+    A = kneighbors_graph(X.astype(np.float32), 15, mode="distance", include_self=False)
+    A.data = np.exp(-A.data / A.data.mean()).astype(np.float32)
+    A = ((A + A.T) * 0.5).tocsr()
+    head, tail, eps = mg.edge_schedule(A, 40)
+    a, b = mg.find_ab_params(1.0, 0.1)
+    Y0 = G.initial_layout(G.pca2(X, 0), 0)
+    outs = []
+    for _ in range(2):
+        Y = Y0.copy()
+        mg.optimize_sgd(Y, head, tail, eps, 40, a=a, b=b, mid_weight=0.1, graph=A, seed=0, parallel="owner")
+        outs.append(Y)
+    assert np.array_equal(outs[0], outs[1])
+    assert np.isfinite(outs[0]).all() and outs[0].shape == (3000, 2)
+    assert KNeighborsClassifier(10).fit(outs[0], y).score(outs[0], y) > 0.95
+    with pytest.raises(ValueError):
+        mg.optimize_sgd(Y0.copy(), head, tail, eps, 40, a=a, b=b, loss=1, parallel="owner")
