@@ -1,12 +1,12 @@
 // Column pass of the FFT repulsion on the in-place engine (fft3.cuh): src/fftconv.cpp:146-186 (forward column
 // transforms, products with the real kernel spectra, inverse column transforms) and the FP64 Z of :226-229.
 //
-// One block per column k of the row half-spectra (persistent over columns). Two shared-memory buffers hold two
-// transforms at once:
-//   phase 1: channels 1 and 2 (x W, y W), each times K2, into outputs 2 and 3;
-//   phase 2: channel 0 (W) once forward; sum K1 |W0h|^2 for Z from its spectrum, and its product with K2 into
-//            output 1. The reference's potential K1 x W0 (output 0) is never formed: Z comes from the spectrum
-//            (Parseval) and the gather reads the potentials 1-3 only.
+// One work item per (column k of the row half-spectra, channel c), persistent blocks, one shared-memory buffer
+// per block (three blocks per SM, so that one block's barriers overlap the others' stages):
+//   channels 1 and 2 (x W, y W): forward, times K2, inverse, into outputs 2 and 3;
+//   channel 0 (W): forward; sum K1 |W0h|^2 for Z from its spectrum, and its product with K2 into output 1. The
+//   reference's potential K1 x W0 (output 0) is never formed: Z comes from the spectrum (Parseval) and the gather
+//   reads the potentials 1-3 only.
 // The first forward stage reads the live rows (g < N) of WhT from global memory, the last inverse stage writes
 // the live rows of PhT, so a column costs 2 (S - 1) shared-memory passes per transform and no reordering pass.
 // Output convention as the one-radix engine: PhT = unnormalised inverse (M x the circular convolution).
@@ -106,7 +106,12 @@ __device__ __forceinline__ double middle2_dispatch(int R, const fft3::Plan& p, f
     }
 }
 
-__global__ void __launch_bounds__(kColThreads, 2) col3_kernel(GridDesc* __restrict__ gd,
+// One (column, channel) per work item, one shared-memory buffer per block: the three channels' convolutions are
+// independent (channel 0 also yields the column's Z share), so a block holds a single transform and the SM
+// holds more blocks to overlap one block's barriers with another's stages.
+constexpr int kColBlocks = 3;   // 3 x 80 registers x 256 threads; 3 buffers of M = 6000 fit the SM
+
+__global__ void __launch_bounds__(kColThreads, kColBlocks) col3_kernel(GridDesc* __restrict__ gd,
                                                               const fft3::Plan* __restrict__ plans,
                                                               const float2* __restrict__ WhT, float2* __restrict__ PhT,
                                                               int Np, int Mhmax, const float* __restrict__ Kt, int Mmax,
@@ -120,58 +125,44 @@ __global__ void __launch_bounds__(kColThreads, 2) col3_kernel(GridDesc* __restri
     if (threadIdx.x == 0) p = plans[M];
     __syncthreads();
     float2* A = sm;
-    float2* B = sm + p.Mp;
     const int S = p.S;
     const int R0 = p.st[0].R, RS = p.st[S - 1].R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = blockIdx.x; k < Mh; k += gridDim.x) {
-        const float2* src[3];
-        float2* dst[4];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) src[c] = WhT + ((size_t)c * Mhmax + k) * Np;
-#pragma unroll
-        for (int o = 0; o < 4; ++o) dst[o] = PhT + ((size_t)o * Mhmax + k) * Np;
+    for (int item = blockIdx.x; item < 3 * Mh; item += gridDim.x) {
+        // channel 0 first for every column, so that the Z shares are ready early
+        const int c = item < Mh ? 0 : (item < 2 * Mh ? 1 : 2);
+        const int k = item - c * Mh;
+        const float2* src = WhT + ((size_t)c * Mhmax + k) * Np;
+        float2* dst = PhT + ((size_t)(c + 1) * Mhmax + k) * Np;
         const float* K1 = Kt + (size_t)k * Mmax;
         const float* K2 = Kt + ((size_t)Mhmax + k) * Mmax;
-        // ---- phase 1: channels 1 and 2, times K2, into outputs 2 and 3
-        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dif_first, p, A, B, 2, ColLoad{src[1], src[2]}, N, tw);
+        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dif_first, p, A, A, 1, ColLoad{src, src}, N, tw);
         __syncthreads();
         for (int s = 1; s < S - 1; ++s) {
-            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dif_mid, p, s, A, B, 2, tw);
+            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dif_mid, p, s, A, A, 1, tw);
             __syncthreads();
         }
-        MGB_FFT3_RADIX_DISPATCH(RS, middle1, p, A, B, 2, K2);
-        __syncthreads();
-        for (int s = S - 2; s >= 1; --s) {
-            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dit_mid, p, s, A, B, 2, tw);
-            __syncthreads();
-        }
-        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dit_last, p, A, B, 2, ColStore{dst[2], dst[3]}, N, tw);
-        __syncthreads();
-        // ---- phase 2: channel 0: Z (sum K1 |W0h|^2) and times K2 into output 1 (the potential K1 x W0 is not
-        // needed: Z comes from the spectrum, and the gather reads the potentials 1-3 only)
-        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dif_first, p, A, B, 1, ColLoad{src[0], src[0]}, N, tw);
-        __syncthreads();
-        for (int s = 1; s < S - 1; ++s) {
-            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dif_mid, p, s, A, B, 1, tw);
-            __syncthreads();
-        }
-        double zs = middle2_dispatch(RS, p, A, K1, K2);
+        if (c == 0) {
+            double zs = middle2_dispatch(RS, p, A, K1, K2);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) zs += __shfl_xor_sync(0xffffffffu, zs, o);
-        if (lane == 0) red[warp] = zs;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-            const bool single = (k == 0) || ((M & 1) == 0 && k == M / 2);
-            zpart[k] = single ? t : 2.0 * t;
-        }
-        for (int s = S - 2; s >= 1; --s) {
-            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dit_mid, p, s, A, B, 1, tw);
+            for (int o = 16; o > 0; o >>= 1) zs += __shfl_xor_sync(0xffffffffu, zs, o);
+            if (lane == 0) red[warp] = zs;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+                const bool single = (k == 0) || ((M & 1) == 0 && k == M / 2);
+                zpart[k] = single ? t : 2.0 * t;
+            }
+        } else {
+            MGB_FFT3_RADIX_DISPATCH(RS, middle1, p, A, A, 1, K2);
             __syncthreads();
         }
-        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dit_last, p, A, B, 1, ColStore{dst[1], dst[1]}, N, tw);
+        for (int s = S - 2; s >= 1; --s) {
+            MGB_FFT3_RADIX_DISPATCH(p.st[s].R, fft3::dit_mid, p, s, A, A, 1, tw);
+            __syncthreads();
+        }
+        MGB_FFT3_RADIX_DISPATCH(R0, fft3::dit_last, p, A, A, 1, ColStore{dst, dst}, N, tw);
         __syncthreads();
     }
     // last block: Z = sum of the partials / M^2 - n
@@ -337,7 +328,8 @@ __global__ void __launch_bounds__(kRowThreads, 2) row_inv3_kernel(const GridDesc
     }
 }
 
-size_t col3_smem(int Mp_max) { return (size_t)2 * Mp_max * sizeof(float2); }
+size_t col3_smem(int Mp_max) { return (size_t)Mp_max * sizeof(float2); }       // one transform per column block
+size_t row3_smem(int Mp_max) { return (size_t)2 * Mp_max * sizeof(float2); }   // two row pairs per row block
 
 }  // namespace
 
@@ -376,7 +368,7 @@ int col3_blocks(int Mp_max) {
 
 // resident blocks of a row kernel (raises its shared-memory limit once per device)
 int row3_blocks(const void* fn, int Mp_max) {
-    const size_t smem = col3_smem(Mp_max);
+    const size_t smem = row3_smem(Mp_max);
     int dev = 0, optin = 0;
     MGB_CUDA(cudaGetDevice(&dev));
     MGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -411,7 +403,7 @@ void fft3_prepare(int Mp_max) {
 void rep_row_fwd3(GridDesc* g, RepBuffers& b, cudaStream_t s) {
     fft3_prepare(b.Mp3max);
     const int blocks = std::min(g_row_blocks.fwd, (b.Nmax + 3) / 4);
-    row_fwd3_kernel<<<blocks, kRowThreads, col3_smem(b.Mp3max), s>>>(
+    row_fwd3_kernel<<<blocks, kRowThreads, row3_smem(b.Mp3max), s>>>(
         g, b.plans3.as<fft3::Plan>(), b.W.as<float4>(), b.Nmax, b.WhT.as<float2>(), b.Npmax, b.Mhmax,
         b.tw.as<float2>());
     MGB_LAUNCH_CHECK();
@@ -420,14 +412,14 @@ void rep_row_fwd3(GridDesc* g, RepBuffers& b, cudaStream_t s) {
 void rep_row_inv3(GridDesc* g, RepBuffers& b, cudaStream_t s) {
     fft3_prepare(b.Mp3max);
     const int blocks = std::min(g_row_blocks.inv, (b.Nmax + 3) / 4);
-    row_inv3_kernel<<<blocks, kRowThreads, col3_smem(b.Mp3max), s>>>(
+    row_inv3_kernel<<<blocks, kRowThreads, row3_smem(b.Mp3max), s>>>(
         g, b.plans3.as<fft3::Plan>(), b.PhT.as<float2>(), b.Npmax, b.Mhmax, b.phi.as<float>(), b.Nmax,
         b.tw.as<float2>());
     MGB_LAUNCH_CHECK();
 }
 
 void rep_col3(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s) {
-    const int blocks = std::min(col3_blocks(b.Mp3max), b.Mhmax);
+    const int blocks = std::min(col3_blocks(b.Mp3max), 3 * b.Mhmax);
     col3_kernel<<<blocks, kColThreads, col3_smem(b.Mp3max), s>>>(
         g, b.plans3.as<fft3::Plan>(), b.WhT.as<float2>(), b.PhT.as<float2>(), b.Npmax, b.Mhmax, b.Kt.as<float>(),
         b.Mmax, b.tw.as<float2>(), b.zpart.as<double>(), n);
