@@ -15,6 +15,7 @@ all host threads) timed on a bounded sample of the same workload (2 SGD epochs a
 2 full-batch iterations at the hybrid pass's grid) and extrapolated to the whole pass.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n N]
+    python bench.py --graph [--n N] [--steps K] [--warmup W] [--no-cpu-baseline]   (the fuzzy neighbour graph)
 """
 import argparse
 import json
@@ -353,6 +354,95 @@ def measured_peak():
         return 6650.0
 
 
+# ----------------------------------------------------------------------------------------------- fuzzy graph
+def graph_bench(n, steps, warmup, cpu_baseline=True):
+    """The fuzzy neighbour graph of the workload (smooth_knn + fuzzy union, magnet/knn.py:215-230) on the device:
+    device-resident passes timed with CUDA events through the C ABI, the package's fuzzy_graph on host arrays
+    (end to end), and the reference's own CPU path (its compiled smooth_knn on all host threads, then the scipy
+    union of magnet/knn.py:221-230) on the same kNN. One JSON line."""
+    import ctypes
+    import torch
+    import scipy.sparse as sp
+    from magnet_b200 import graph as G
+    X, _ = make_data(n, seed=2)
+    ind, dist = G.exact_knn(X, 15)
+    ind = np.ascontiguousarray(ind, dtype=np.int32)
+    dist = np.ascontiguousarray(dist, dtype=np.float32)
+    k = ind.shape[1]
+    lib = ctypes.CDLL(os.path.join(ROOT, "lib-magnet_b200", "libmagnet_b200.so"))
+    P_, I64 = ctypes.c_void_p, ctypes.c_int64
+    lib.mg_smooth_knn.argtypes = [P_, I64, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, P_]
+    lib.mg_fuzzy_union.argtypes = [P_, P_, I64, ctypes.c_int, I64, ctypes.c_double, P_, P_, P_, I64,
+                                   ctypes.POINTER(I64)]
+    lib.mg_launch_count.restype = ctypes.c_uint64
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dd, idd = torch.from_numpy(dist).to(dev), torch.from_numpy(ind).to(dev)
+    vd = torch.empty_like(dd)
+    cap = 2 * n * k
+    ipd = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    ixd = torch.empty(cap, dtype=torch.int32, device=dev)
+    dtd = torch.empty(cap, dtype=torch.float32, device=dev)
+    nnz = I64(0)
+
+    def device_pass():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        if lib.mg_smooth_knn(dd.data_ptr(), n, k, 15, 1.0, 64, vd.data_ptr()) != 0:
+            raise RuntimeError("mg_smooth_knn failed")
+        ev[1].record()
+        if lib.mg_fuzzy_union(idd.data_ptr(), vd.data_ptr(), n, k, n, 1.0, ipd.data_ptr(), ixd.data_ptr(),
+                              dtd.data_ptr(), cap, ctypes.byref(nnz)) != 0:
+            raise RuntimeError("mg_fuzzy_union failed")
+        ev[2].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+
+    for _ in range(warmup):
+        device_pass()
+    l0 = lib.mg_launch_count()
+    times = [device_pass() for _ in range(steps)]
+    launches = int(lib.mg_launch_count() - l0) // max(steps, 1)
+    smooth_ms = statistics.median(t[0] for t in times)
+    union_ms = statistics.median(t[1] for t in times)
+    e2e_s = float("inf")
+    for _ in range(2):   # the first call also sizes the staging buffers
+        t0 = time.perf_counter()
+        P = G.fuzzy_graph(ind, dist, 15)
+        e2e_s = min(e2e_s, time.perf_counter() - t0)
+    out = {"metric": "fuzzy neighbour graph (smooth_knn + union) ms", "n": n, "k": k, "nnz": int(nnz.value),
+           "value": round(smooth_ms + union_ms, 3), "unit": "ms", "smooth_knn_ms": round(smooth_ms, 3),
+           "union_ms": round(union_ms, 3), "e2e": {"value": round(e2e_s * 1e3, 2), "unit": "ms"},
+           "gpu_launches": launches, "steps": steps, "warmup": warmup, "higher_is_better": False,
+           "data": "synthetic", "config": {"workload": "15-NN fuzzy graph of the hybrid workload's data (n=%d, d=50, "
+                                                       "100 anisotropic Gaussians, seed 2), exact kNN" % n}}
+    if cpu_baseline:
+        from oracle import oracle as O
+        R = O.reference()
+        if R is not None:
+            t0 = time.perf_counter()
+            vals = np.asarray(R.smooth_knn(dist, 15, 1.0, 64, -1))
+            t1 = time.perf_counter()
+            rows = np.repeat(np.arange(n, dtype=np.int64), k)
+            A = sp.csr_matrix((vals.ravel(), (rows, ind.ravel())), shape=(n, n), dtype=np.float32)
+            A.eliminate_zeros()
+            T = A.T.tocsr()
+            prod = A.multiply(T)
+            Pr = (1.0 * (A + T - prod) + 0.0 * prod).tocsr()
+            Pr.eliminate_zeros()
+            Pr.sort_indices()
+            t2 = time.perf_counter()
+            out["cpu_baseline"] = {"value": round((t2 - t0) * 1e3, 1), "unit": "ms", "cores": os.cpu_count(),
+                                   "kind": "reference", "smooth_knn_ms": round((t1 - t0) * 1e3, 1),
+                                   "union_ms": round((t2 - t1) * 1e3, 1),
+                                   "sample": "the whole graph: the reference's compiled smooth_knn on all host "
+                                             "threads, then magnet/knn.py's scipy union"}
+            out["parity"] = {"pattern_equal": bool(np.array_equal(P.indptr, Pr.indptr)
+                                                   and np.array_equal(P.indices, Pr.indices)),
+                             "max_abs_diff": float(np.abs(P.data - Pr.data).max())}
+    print(json.dumps(out), flush=True)
+
+
 # ----------------------------------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -362,7 +452,13 @@ def main():
     ap.add_argument("--impl", default="magnet_b200", choices=["magnet_b200", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graph", action="store_true", help="time the fuzzy neighbour graph instead of the layout")
     args = ap.parse_args()
+    if args.graph:
+        import torch
+        torch.cuda.set_device(0)
+        graph_bench(args.n, args.steps, args.warmup, not args.no_cpu_baseline)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -178,6 +178,20 @@ int mg_optimize_layout(const mg_layout_args* a);
 int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* sampled, int32_t* n_neg, int64_t* neg_off,
                        int32_t* negs, int64_t negs_cap, int64_t* n_negs, int32_t* mid);
 
+/* ================================================================ fuzzy neighbour graph
+ * smooth_knn (src/graph.cpp:29-78, bound at src/bindings.cpp:73-74): dist (n, k) sorted distances to the
+ * neighbours (self excluded) -> out (n, k) memberships in (0, 1]; the bisection of each row's bandwidth to
+ * log2(n_neighbors) * bandwidth in n_iter steps at most. */
+int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter, float* out);
+
+/* The fuzzy union of fuzzy_graph (magnet/knn.py:215-230, after smooth_knn): A = the n x n matrix with rows
+ * i < n_rows holding (ind[i, j], vals[i, j]) (duplicate columns summed, zeros dropped), and
+ * P = mix (A + A^T - A o A^T) + (1 - mix) (A o A^T) with mix = set_op_mix_ratio, zeros dropped, columns sorted.
+ * Outputs indptr (n + 1), indices / data of capacity cap (2 n_rows k always suffices); *nnz = entries. An index
+ * outside [0, n) is MG_ERR_ARGUMENT. */
+int mg_fuzzy_union(const int32_t* ind, const float* vals, int64_t n_rows, int k, int64_t n, double set_op_mix_ratio,
+                   int32_t* indptr, int32_t* indices, float* data, int64_t cap, int64_t* nnz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,8 +2,8 @@
 
 Put the directory holding this package ahead of the reference's extension on sys.path; the reference's Python
 package (`magnet`) then runs its layout pass on the B200: optimize_layout, FFTConv2D, tsne_attraction, tsne_step,
-tsne_update, bbox_2d and mid_spring come from the device library. The host-side kernels that stay on the
-reference's code (nn_descent, knn_search, smooth_knn, mid-near pairs, spectral init, louvain) are forwarded to
+tsne_update, bbox_2d, mid_spring and smooth_knn come from the device library. The host-side kernels that stay on
+the reference's code (nn_descent, knn_search, mid-near pairs, spectral init, louvain) are forwarded to
 the reference's own compiled module, found through the MAGNET_HOST_MODULE environment variable (path to the
 reference's `_magnet*.so`); without it they raise ImportError when used, as a missing `_magnet` would.
 """
@@ -11,12 +11,11 @@ import importlib.util as _ilu
 import os as _os
 
 from magnet_b200._native import (FFTConv2D, optimize_layout, tsne_attraction, tsne_step, tsne_update,  # noqa: F401
-                                 bbox_2d, mid_spring)
+                                 bbox_2d, mid_spring, smooth_knn)
 
-_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search", "knn_search_sparse", "smooth_knn",
-               "mid_near_pairs_dense", "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration",
-               "louvain", "interp_scatter", "interp_gather", "scatter_padded_2d", "spectral_products",
-               "gather_forces_2d", "umap_attraction")
+_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search", "knn_search_sparse", "mid_near_pairs_dense",
+               "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration", "louvain", "interp_scatter",
+               "interp_gather", "scatter_padded_2d", "spectral_products", "gather_forces_2d", "umap_attraction")
 
 
 def _load_host():

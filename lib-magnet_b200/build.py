@@ -23,8 +23,9 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
 
-# per-file flags: owner mode rounds every product and sum on its own, as the reference's plain x86-64 build
-FILE_FLAGS = {"owner.cu": ["-fmad=false"]}
+# per-file flags: owner mode and the graph passes round every product and sum on their own, as the reference's
+# plain x86-64 build and numpy do
+FILE_FLAGS = {"owner.cu": ["-fmad=false"], "graph.cu": ["-fmad=false"]}
 
 
 def _newer(target, deps):

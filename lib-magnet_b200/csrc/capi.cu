@@ -5,6 +5,7 @@
 #include "fft.cuh"
 #include "tsne.cuh"
 #include "sgd.cuh"
+#include "graph.cuh"
 #include <string>
 #include <vector>
 #include <memory>
@@ -644,3 +645,55 @@ extern "C" int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* s
         MGB_CUDA(cudaStreamSynchronize(s));
     });
 }
+
+// ================================================================ fuzzy neighbour graph
+namespace {
+thread_local std::unique_ptr<GraphWork> g_graph_work;
+GraphWork& graph_work() {
+    if (!g_graph_work) g_graph_work.reset(new GraphWork());
+    return *g_graph_work;
+}
+}  // namespace
+
+extern "C" int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter,
+                             float* out) {
+    return guard([&] {
+        require(n >= 0 && k >= 0 && (n * (int64_t)k == 0 || (dist && out)), "dist must be (n, k)");
+        require(n_neighbors >= 1, "n_neighbors must be positive");
+        cudaStream_t s = current_stream();
+        // src/graph.cpp:35, on the host libm as the reference evaluates it
+        const float target = std::log2((float)n_neighbors) * bandwidth;
+        const float* d = in_dev(dist, n * k, 0, s);
+        float* o = out_dev(out, n * k, 1);
+        smooth_knn_dev(d, n, k, target, n_iter, o, graph_work(), s);
+        back(out, o, n * k, s);
+        if (any_host({dist, out})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" int mg_fuzzy_union(const int32_t* ind, const float* vals, int64_t n_rows, int k, int64_t n,
+                              double set_op_mix_ratio, int32_t* indptr, int32_t* indices, float* data, int64_t cap,
+                              int64_t* nnz) {
+    return guard([&] {
+        require(n_rows >= 0 && k >= 0 && n >= n_rows, "ind must be (n_rows, k) with n_rows <= n");
+        require(n_rows * (int64_t)k == 0 || (ind && vals), "ind and vals must not be NULL");
+        require(indptr && nnz && cap >= 0 && (cap == 0 || (indices && data)), "outputs must not be NULL");
+        require(n <= INT32_MAX, "n must fit 32-bit indices");
+        cudaStream_t s = current_stream();
+        const int32_t* id = in_dev(ind, n_rows * k, 0, s);
+        const float* vd = in_dev(vals, n_rows * k, 1, s);
+        int32_t* ipd = out_dev(indptr, n + 1, 2);
+        int32_t* ixd = out_dev(indices, cap, 3);
+        float* dd = out_dev(data, cap, 4);
+        // scipy multiplies the float32 arrays by the python floats mix and 1 - mix as float32 scalars
+        const float mix = (float)set_op_mix_ratio;
+        const float one_minus_mix = (float)(1.0 - set_op_mix_ratio);
+        const int64_t m = fuzzy_union_dev(id, vd, n_rows, k, n, mix, one_minus_mix, ipd, ixd, dd, cap, graph_work(), s);
+        back(indptr, ipd, n + 1, s);
+        back(indices, ixd, m, s);
+        back(data, dd, m, s);
+        *nnz = m;
+        MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+

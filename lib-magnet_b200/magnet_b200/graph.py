@@ -1,11 +1,10 @@
 """Host-side inputs of the layout pass: the fuzzy neighbour graph, mid-near partners and the initial layout.
 
-These steps are upstream of the layout pass; the reference runs them on the host (NN-descent, smooth kNN,
-fuzzy union, mid-near pairs, spectral / PCA init) and so does this package. They are restated here, from the
-reference's behaviour, so that workloads can be built where the reference is not installed:
+These steps are upstream of the layout pass. The fuzzy graph runs on the device; the others are restated here
+on the host, from the reference's behaviour, so that workloads can be built where the reference is not installed:
 
-* ``smooth_knn``: UMAP's per-row bandwidth search (src/graph.cpp:29-78, magnet/knn.py:165-198);
-* ``fuzzy_graph``: the fuzzy union A + A^T - A o A^T (magnet/knn.py:215-230);
+* ``smooth_knn``: UMAP's per-row bandwidth search (src/graph.cpp:29-78), on the device;
+* ``fuzzy_graph``: the fuzzy union A + A^T - A o A^T (magnet/knn.py:215-230), on the device;
 * ``exact_knn``: exact k nearest neighbours (self excluded, sorted) by blocked matmul on a CUDA device when
   torch sees one, else numpy; it stands in for NN-descent (src/nndescent.cpp), whose output it bounds;
 * ``mid_near_pairs``: PaCMAP-style partners, the second closest of n_cand random rows (src/nndescent.cpp:731-759);
@@ -16,56 +15,37 @@ import scipy.sparse as sp
 
 
 def smooth_knn(dist, n_neighbors, bandwidth=1.0, n_iter=64):
-    """dist (n, k) sorted neighbour distances (self excluded) -> memberships (n, k) in (0, 1]; vectorised over rows,
-    float32 as the reference's kernel."""
+    """dist (n, k) sorted neighbour distances (self excluded) -> memberships (n, k) in (0, 1], on the device
+    (src/graph.cpp:29-78)"""
+    from . import _native
+    return _native.smooth_knn(np.ascontiguousarray(dist, dtype=np.float32), int(n_neighbors), float(bandwidth),
+                              int(n_iter))
+
+
+def rescale_neighbor_distances(dist, power=1.0, rank_exponent=0.0):
+    """the distance-profile reshaping of magnet/knn.py:201-213: d_k <- d_1 (d_k / d_1)^power, then
+    d_k <- d_k k^rank_exponent"""
     dist = np.asarray(dist, dtype=np.float32)
-    n, k = dist.shape
-    target = np.float32(np.log2(np.float32(n_neighbors)) * np.float32(bandwidth))
-    nonzero = dist > 0
-    has = nonzero.any(1)
-    first = np.argmax(nonzero, axis=1)
-    rho = np.where(has, dist[np.arange(n), first], np.float32(0)).astype(np.float32)
-    dmr = dist - rho[:, None]
-    lo = np.zeros(n, np.float32)
-    hi = np.full(n, np.inf, np.float32)
-    mid = np.ones(n, np.float32)
-    sigma = np.ones(n, np.float32)
-    done = np.zeros(n, bool)
-    for _ in range(n_iter):
-        psum = np.where(dmr > 0, np.exp(-dmr / mid[:, None]), np.float32(1)).astype(np.float32).sum(1, dtype=np.float32)
-        newly = (~done) & (np.abs(psum - target) < 1e-5)
-        sigma[newly] = mid[newly]
-        done |= newly
-        if done.all():
-            break
-        gt = psum > target
-        hi = np.where(done, hi, np.where(gt, mid, hi))
-        lo = np.where(done, lo, np.where(gt, lo, mid))
-        mid = np.where(done, mid, np.where(gt, (lo + hi) * np.float32(0.5),
-                                           np.where(np.isinf(hi), mid * np.float32(2), (lo + hi) * np.float32(0.5))))
-        mid = mid.astype(np.float32)
-    sigma[~done] = mid[~done]
-    mean_row = dist.astype(np.float64).sum(1) / k
-    sigma = np.where(rho > 0, np.maximum(sigma, np.float32(1e-3) * mean_row.astype(np.float32)), sigma)
-    mean_all = np.float32(dist.astype(np.float64).sum() / (n * k))
-    sigma = np.where(rho > 0, sigma, np.maximum(sigma, np.float32(1e-3) * mean_all)).astype(np.float32)
-    return np.where(dmr > 0, np.exp(-dmr / sigma[:, None]), np.float32(1)).astype(np.float32)
+    if power != 1.0:
+        d1 = np.maximum(dist[:, :1], 1e-12)
+        dist = d1 * (np.maximum(dist, 0.0) / d1) ** power
+    if rank_exponent != 0.0:
+        dist = dist * (np.arange(1, dist.shape[1] + 1, dtype=np.float32) ** rank_exponent)[None, :]
+    return dist.astype(np.float32)
 
 
-def fuzzy_graph(ind, dist, n_neighbors, n=None, set_op_mix_ratio=1.0):
-    """symmetric fuzzy neighbourhood graph (CSR float32, sorted indices, no diagonal)"""
-    n = ind.shape[0] if n is None else n
+def fuzzy_graph(ind, dist, n_neighbors, n=None, set_op_mix_ratio=1.0, power=1.0, rank_exponent=0.0):
+    """symmetric fuzzy neighbourhood graph (CSR float32, sorted indices) from kNN indices and distances
+    (magnet/knn.py:215-230): smooth_knn memberships and the union A + A^T - A o A^T, both on the device"""
+    from . import _native
+    n = ind.shape[0] if n is None else int(n)
+    if power != 1.0 or rank_exponent != 0.0:
+        dist = rescale_neighbor_distances(dist, power, rank_exponent)
     vals = smooth_knn(dist, n_neighbors)
-    rows = np.repeat(np.arange(n, dtype=np.int64), ind.shape[1])
-    A = sp.csr_matrix((vals.ravel(), (rows, np.asarray(ind).ravel())), shape=(n, n), dtype=np.float32)
-    A.eliminate_zeros()
-    T = A.T.tocsr()
-    prod = A.multiply(T)
-    P = set_op_mix_ratio * (A + T - prod) + (1.0 - set_op_mix_ratio) * prod
-    P = sp.csr_matrix(P, dtype=np.float32)
-    P.setdiag(0)
-    P.eliminate_zeros()
-    P.sort_indices()
+    indptr, indices, data = _native.fuzzy_union(np.ascontiguousarray(ind, dtype=np.int32), vals, n,
+                                                float(set_op_mix_ratio))
+    P = sp.csr_matrix((data, indices, indptr), shape=(n, n))
+    P.has_sorted_indices = True
     return P
 
 

@@ -231,6 +231,42 @@ py::tuple layout_schedule(py::object Y, py::object head, py::object tail, py::ob
     return py::make_tuple(sampled, n_neg, off, negs[py::slice(0, tot, 1)], mid);
 }
 
+// smooth_knn of src/graph.cpp:29-78 on the device (signature of src/bindings.cpp:73-74)
+py::array_t<float> smooth_knn(py::object dist, int n_neighbors, float bandwidth, int n_iter, int n_threads) {
+    (void)n_threads;
+    auto d = view<float>(dist);
+    if (d.ndim() != 2) throw std::runtime_error("dist must be (n, k)");
+    const int64_t n = d.dim(0);
+    const int k = (int)d.dim(1);
+    py::array_t<float> out({n, (int64_t)k});
+    {
+        py::gil_scoped_release rel;
+        check(mg_smooth_knn(d.ptr, n, k, n_neighbors, bandwidth, n_iter, out.mutable_data()));
+    }
+    return out;
+}
+
+// the fuzzy union of magnet/knn.py:221-230 on the device: (indptr, indices, data) of the n x n CSR
+py::tuple fuzzy_union(py::object ind, py::object vals, int64_t n, double set_op_mix_ratio) {
+    auto id = view<int32_t>(ind);
+    auto v = view<float>(vals);
+    if (id.ndim() != 2 || v.ndim() != 2 || id.dim(0) != v.dim(0) || id.dim(1) != v.dim(1))
+        throw std::runtime_error("ind and vals must be (n, k) of the same shape");
+    const int64_t rows = id.dim(0);
+    const int k = (int)id.dim(1);
+    if (n < 0) n = rows;
+    const int64_t cap = std::max<int64_t>(2 * rows * k, 1);
+    py::array_t<int32_t> indptr(n + 1), indices(cap);
+    py::array_t<float> data(cap);
+    int64_t nnz = 0;
+    {
+        py::gil_scoped_release rel;
+        check(mg_fuzzy_union(id.ptr, v.ptr, rows, k, n, set_op_mix_ratio, indptr.mutable_data(),
+                             indices.mutable_data(), data.mutable_data(), cap, &nnz));
+    }
+    return py::make_tuple(indptr, indices[py::slice(0, nnz, 1)], data[py::slice(0, nnz, 1)]);
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_native, m) {
@@ -263,6 +299,11 @@ PYBIND11_MODULE(_native, m) {
           py::arg("indptr") = py::none(), py::arg("indices") = py::none(), py::arg("seed") = 0,
           py::arg("stream_mode") = 0, py::arg("walk_lens") = py::none(), py::arg("jump_indptr") = py::none(),
           py::arg("jump_indices") = py::none(), py::arg("mid_jump") = 0.0f);
+    m.def("smooth_knn", &smooth_knn, "UMAP smooth-kNN memberships (n, k) from sorted neighbour distances (device)",
+          py::arg("dist"), py::arg("n_neighbors"), py::arg("bandwidth") = 1.0f, py::arg("n_iter") = 64,
+          py::arg("n_threads") = -1);
+    m.def("fuzzy_union", &fuzzy_union, "fuzzy union A + A^T - A o A^T of kNN memberships (device): (indptr, indices, data)",
+          py::arg("ind"), py::arg("vals"), py::arg("n") = -1, py::arg("set_op_mix_ratio") = 1.0);
     m.def("tsne_attraction", [](py::object indptr, py::object indices, py::object data, py::object Y, float dof, int) {
               auto ip = view<int32_t>(indptr), ix = view<int32_t>(indices);
               auto P = view<float>(data);

@@ -16,6 +16,8 @@
  *   orc_sgd_schedule    the draws epoch_worker makes (src/layout.cpp:123,135,160-166,184,226-249), recorded
  *                       instead of applied; one stream per epoch (tid 0, the n_threads=1 reference), or the
  *                       device fast mode's counter draws (each draw of a sample addressed by edge and index)
+ *   orc_smooth_knn      src/graph.cpp:29-78 (one thread: the whole array's mean is one sequential FP64 sum)
+ *   orc_fuzzy_union     magnet/knn.py:221-230 (scipy's csr construction, transpose, A + T - A o T, mix), float32
  *   orc_spread / orc_gather  src/fftconv.cpp:24-40 (lagrange_w), :83-123 (spread), :200-229 (gather)
  *   orc_tsne_attraction src/fftrep.cpp:129-177
  *   orc_tsne_step       src/fftrep.cpp:225-266 (one thread: nt = 1 partial sums, i.e. blocks of 1024 rows)
@@ -504,6 +506,110 @@ int orc_sgd_owner(orc_sgd_args* c, const int32_t* rev_indptr, const int32_t* rev
     }
     free(Yr); free(own); free(eown);
     return 0;
+}
+
+/* ------------------------------------------------------------------ fuzzy neighbour graph */
+/* smooth_knn (src/graph.cpp:29-78) on one thread: the row's FP64 distance sum and rho (first positive
+ * distance), the bisection of sigma (at most n_iter steps, stop within 1e-5 of log2(n_neighbors) * bandwidth),
+ * the floor 1e-3 x the row's mean distance (the whole array's when rho = 0), then the memberships. */
+void orc_smooth_knn(const float* D, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter, float* out) {
+    const float target = log2f((float)n_neighbors) * bandwidth;
+    float* sigma = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* rho = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    double tot = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const float* d = D + i * k;
+        double rowsum = 0.0; float r = 0.f; int has = 0;
+        for (int j = 0; j < k; ++j) { rowsum += d[j]; if (!has && d[j] > 0.f) { r = d[j]; has = 1; } }
+        tot += rowsum;
+        rho[i] = r;
+        float lo = 0.f, hi = INFINITY, mid = 1.f, sg = 1.f; int done = 0;
+        for (int it = 0; it < n_iter; ++it) {
+            float psum = 0.f;
+            for (int j = 0; j < k; ++j) { const float dmr = d[j] - r; psum += dmr > 0.f ? expf(-dmr / mid) : 1.f; }
+            if (fabsf(psum - target) < 1e-5f) { sg = mid; done = 1; break; }
+            if (psum > target) { hi = mid; mid = (lo + hi) * 0.5f; }
+            else { lo = mid; mid = isinf(hi) ? mid * 2.f : (lo + hi) * 0.5f; }
+        }
+        if (!done) sg = mid;
+        const float mean_row = (float)(rowsum / k);
+        if (r > 0.f) sg = fmaxf(sg, 1e-3f * mean_row);
+        sigma[i] = sg;
+    }
+    const float mean_all = (float)(tot / (double)(n * k));
+    for (int64_t i = 0; i < n; ++i) {
+        const float* d = D + i * k; float* o = out + i * k;
+        float sg = sigma[i];
+        if (!(rho[i] > 0.f)) sg = fmaxf(sg, 1e-3f * mean_all);
+        for (int j = 0; j < k; ++j) { const float dmr = d[j] - rho[i]; o[j] = dmr > 0.f ? expf(-dmr / sg) : 1.f; }
+    }
+    free(sigma); free(rho);
+}
+
+/* The fuzzy union of magnet/knn.py:221-230 with scipy's float32 arithmetic: A = csr((vals, (rows, ind))) with
+ * duplicate columns summed (in row order) and zeros dropped; T = A^T; per entry (a, t):
+ * both: d = (a + t) - a t, P = d mix + (a t) (1 - mix); one: P = x mix; zeros dropped, columns sorted.
+ * mix and 1 - mix are the float32 roundings of the python floats. Returns nnz (entries beyond cap are not
+ * written), or -1 for an index outside [0, n). */
+int64_t orc_fuzzy_union(const int32_t* ind, const float* vals, int64_t n_rows, int k, int64_t n, double mix_d,
+                        int32_t* indptr, int32_t* indices, float* data, int64_t cap) {
+    const float mix = (float)mix_d, omm = (float)(1.0 - mix_d);
+    const size_t ek = (size_t)(n_rows * k > 0 ? n_rows * k : 1);
+    int32_t* ac = (int32_t*)malloc(sizeof(int32_t) * ek); float* av = (float*)malloc(sizeof(float) * ek);
+    int32_t* al = (int32_t*)calloc((size_t)(n_rows > 0 ? n_rows : 1), sizeof(int32_t));
+    int64_t* tp = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+    int32_t* tr = (int32_t*)malloc(sizeof(int32_t) * ek); float* tv = (float*)malloc(sizeof(float) * ek);
+    int64_t nnz = 0;
+    for (int64_t i = 0; i < n_rows; ++i) {
+        int32_t* c = ac + i * k; float* v = av + i * k;
+        for (int j = 0; j < k; ++j) {
+            const int32_t col = ind[i * k + j];
+            if (col < 0 || col >= n) { nnz = -1; goto done; }
+            int p = j;
+            while (p > 0 && c[p - 1] > col) { c[p] = c[p - 1]; v[p] = v[p - 1]; --p; }
+            c[p] = col; v[p] = vals[i * k + j];
+        }
+        int m = 0;
+        for (int j = 0; j < k;) {
+            const int32_t col = c[j]; float x = v[j]; int e = j + 1;
+            for (; e < k && c[e] == col; ++e) x += v[e];
+            if (x != 0.f) { c[m] = col; v[m] = x; ++m; }
+            j = e;
+        }
+        al[i] = m;
+    }
+    /* T by a stable counting sort on the column: rows come out in increasing order */
+    for (int64_t i = 0; i < n_rows; ++i) for (int j = 0; j < al[i]; ++j) tp[ac[i * k + j] + 1]++;
+    for (int64_t r = 0; r < n; ++r) tp[r + 1] += tp[r];
+    {
+        int64_t* cur = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+        for (int64_t r = 0; r < n; ++r) cur[r] = tp[r];
+        for (int64_t i = 0; i < n_rows; ++i)
+            for (int j = 0; j < al[i]; ++j) { const int32_t col = ac[i * k + j]; tr[cur[col]] = (int32_t)i; tv[cur[col]] = av[i * k + j]; cur[col]++; }
+        free(cur);
+    }
+    indptr[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int la = i < n_rows ? al[i] : 0;
+        const int32_t* c = ac + i * k; const float* v = av + i * k;
+        int ja = 0; int64_t ta = tp[i];
+        while (ja < la || ta < tp[i + 1]) {
+            const int32_t ca = ja < la ? c[ja] : INT32_MAX, ct = ta < tp[i + 1] ? tr[ta] : INT32_MAX;
+            const int32_t col = ca < ct ? ca : ct;
+            float x;
+            if (ca == col && ct == col) {
+                const float a = v[ja], t = tv[ta], prod = a * t, d = (a + t) - prod;
+                x = d * mix + prod * omm;
+                ++ja; ++ta;
+            } else if (ca == col) { x = v[ja] * mix; ++ja; }
+            else { x = tv[ta] * mix; ++ta; }
+            if (x != 0.f) { if (nnz < cap) { indices[nnz] = col; data[nnz] = x; } ++nnz; }
+        }
+        indptr[i + 1] = (int32_t)nnz;
+    }
+done:
+    free(ac); free(av); free(al); free(tp); free(tr); free(tv);
+    return nnz;
 }
 
 /* ------------------------------------------------------------------ FFT repulsion pieces (src/fftconv.cpp) */

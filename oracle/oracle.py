@@ -84,6 +84,9 @@ def lib():
         L.orc_sgd_owner.restype = ctypes.c_int
         L.orc_owner_chunks.argtypes = [_P, _I64, _I64, _P, _P]
         L.orc_owner_chunks.restype = ctypes.c_int
+        L.orc_smooth_knn.argtypes = [_P, _I64, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _P]
+        L.orc_fuzzy_union.argtypes = [_P, _P, _I64, ctypes.c_int, _I64, ctypes.c_double, _P, _P, _P, _I64]
+        L.orc_fuzzy_union.restype = _I64
         L.orc_sgd_schedule.argtypes = [ctypes.POINTER(SgdArgs), ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _I64, _P]
         L.orc_sgd_schedule.restype = _I64
         L.orc_spread.argtypes = [_P, _I64, _F, _F, _F, ctypes.c_int, ctypes.c_int, _P]
@@ -210,6 +213,31 @@ def sgd_schedule(Y, head, tail, eps, eons, eonns, epoch, per_edge_stream=False, 
                                  n_neg.ctypes.data, neg_off.ctypes.data, negs.ctypes.data, cap, mid.ctypes.data)
     assert tot <= cap, "negative buffer too small"
     return sampled, n_neg, neg_off, negs[:tot], mid
+
+
+# ---------------------------------------------------------------------------------------------- fuzzy graph
+def smooth_knn(dist, n_neighbors, bandwidth=1.0, n_iter=64):
+    """src/graph.cpp:29-78 on one host thread: memberships (n, k) float32"""
+    dist = _c32(dist, np.float32)
+    n, k = dist.shape
+    out = np.empty_like(dist)
+    lib().orc_smooth_knn(dist.ctypes.data, n, k, int(n_neighbors), float(bandwidth), int(n_iter), out.ctypes.data)
+    return out
+
+
+def fuzzy_union(ind, vals, n=None, set_op_mix_ratio=1.0):
+    """the union of magnet/knn.py:221-230 given the memberships: (indptr, indices, data) of the n x n CSR"""
+    ind = _c32(ind, np.int32)
+    vals = _c32(vals, np.float32)
+    rows, k = ind.shape
+    n = rows if n is None else int(n)
+    cap = max(2 * rows * k, 1)
+    indptr = np.zeros(n + 1, np.int32); indices = np.zeros(cap, np.int32); data = np.zeros(cap, np.float32)
+    nnz = lib().orc_fuzzy_union(ind.ctypes.data, vals.ctypes.data, rows, k, n, float(set_op_mix_ratio),
+                                indptr.ctypes.data, indices.ctypes.data, data.ctypes.data, cap)
+    if nnz < 0:
+        raise ValueError("neighbour index out of range")
+    return indptr, indices[:nnz], data[:nnz]
 
 
 # ---------------------------------------------------------------------------------------------- t-SNE kernels

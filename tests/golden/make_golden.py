@@ -2,11 +2,11 @@
 
 Runs only where the reference checkout is available (default /root/reference, override with
 MAGNET_REFERENCE_DIR) and its native module has been compiled by oracle/build_ref.sh. Every output is produced
-by the reference's own code: its compiled `_magnet` (optimize_layout at n_threads=1, FFTConv2D, tsne_attraction,
-tsne_step, bbox_2d) and its Python drivers (magnet/tsne.py FFTRepulsion2D / optimize_tsne, magnet/knn.py
-fuzzy_graph, magnet/__init__.py edge schedule). Inputs are seeded synthetic data.
+by the reference's own code: its compiled `_magnet` (optimize_layout at n_threads=1 and in owner mode, FFTConv2D,
+tsne_attraction, tsne_step, bbox_2d, smooth_knn) and its Python drivers (magnet/tsne.py FFTRepulsion2D /
+optimize_tsne, magnet/knn.py fuzzy_graph, magnet/__init__.py edge schedule). Inputs are seeded synthetic data.
 
-    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner]
+    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner graph]
 """
 import os
 import sys
@@ -171,6 +171,35 @@ def sgd_options_fixture():
     np.savez_compressed(os.path.join(HERE, "sgd_options.npz"), **out)
 
 
+def graph_fixture():
+    """the reference's smooth_knn (compiled) and fuzzy_graph (magnet/knn.py) on the 600-point blobs' exact 15-NN
+    (self excluded): the default union, set_op_mix_ratio 0.5, rank_exponent 0.25, and an edge case with duplicate
+    neighbours, all-zero distance rows, a zero first distance and rows whose far memberships underflow to 0"""
+    from magnet.knn import fuzzy_graph as ref_fuzzy_graph
+    X = dict(np.load(os.path.join(HERE, "sgd_small.npz")))["X"]
+    D = ((X[:, None, :].astype(np.float64) - X[None, :, :]) ** 2).sum(-1)
+    np.fill_diagonal(D, np.inf)
+    ind = np.argsort(D, 1, kind="stable")[:, :14].astype(np.int32)
+    dist = np.sqrt(np.take_along_axis(D, ind, 1)).astype(np.float32)
+    ind_e, dist_e = ind.copy(), dist.copy()
+    ind_e[0:10, 5] = ind_e[0:10, 4]
+    dist_e[10:20] = 0.0
+    dist_e[20:30, 0] = 0.0
+    dist_e[30:40, :5] = 1.0
+    dist_e[30:40, 5:] = 1000.0
+    out = dict(ind=ind, dist=dist, ind_e=ind_e, dist_e=dist_e)
+    cases = {"": (ind, dist, {}), "_mix": (ind, dist, dict(set_op_mix_ratio=0.5)),
+             "_rank": (ind, dist, dict(rank_exponent=0.25)), "_e": (ind_e, dist_e, {})}
+    for suffix, (ii, dd, kw) in cases.items():
+        P = ref_fuzzy_graph(ii, dd, 15, **kw)
+        out["indptr" + suffix] = P.indptr.astype(np.int32)
+        out["indices" + suffix] = P.indices.astype(np.int32)
+        out["data" + suffix] = P.data.astype(np.float32)
+    out["vals"] = np.asarray(_magnet.smooth_knn(dist, 15))
+    out["vals_e"] = np.asarray(_magnet.smooth_knn(dist_e, 15))
+    np.savez_compressed(os.path.join(HERE, "graph_small.npz"), **out)
+
+
 def sgd_owner_fixture():
     """the reference's owner mode (parallel=1, 4 threads; its result does not depend on the thread count) on each
     owner case of sgd_cases.py: the final Y and sha-256 digests of eons, eonns and the Adam state at seed 12345,
@@ -197,10 +226,10 @@ def sgd_owner_fixture():
 
 if __name__ == "__main__":
     # all fixtures, or only those named on the command line (sgd_options reads sgd_small.npz)
-    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner"]
+    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner", "graph"]
     for name in todo:
         {"sgd": sgd_fixture, "fft": fft_fixture, "tsne": tsne_fixture, "sgd_options": sgd_options_fixture,
-         "sgd_owner": sgd_owner_fixture}[name]()
+         "sgd_owner": sgd_owner_fixture, "graph": graph_fixture}[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

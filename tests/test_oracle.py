@@ -97,6 +97,21 @@ def test_owner_chunks_follow_edge_quantiles(big_graph):
         assert eown[t] == np.searchsorted(head, own[t], "left")
 
 
+def test_graph_oracle_bit_exact(golden):
+    """smooth_knn and the fuzzy union restated in C equal the reference's compiled smooth_knn and its
+    magnet/knn.py fuzzy_graph bit for bit (graph_small.npz): the default union, set_op_mix_ratio 0.5, and rows with
+    duplicate neighbours, all-zero distances, a zero first distance and memberships that underflow to 0"""
+    g = golden("graph_small.npz")
+    assert np.array_equal(O.smooth_knn(g["dist"], 15), g["vals"])
+    vals_e = O.smooth_knn(g["dist_e"], 15)
+    assert np.array_equal(vals_e, g["vals_e"]) and (vals_e == 0).sum() > 0
+    for suffix, ind, vals, mix in (("", g["ind"], g["vals"], 1.0), ("_mix", g["ind"], g["vals"], 0.5),
+                                   ("_e", g["ind_e"], g["vals_e"], 1.0)):
+        indptr, indices, data = O.fuzzy_union(ind, vals, None, mix)
+        assert np.array_equal(indptr, g["indptr" + suffix]) and np.array_equal(indices, g["indices" + suffix])
+        assert np.array_equal(data, g["data" + suffix])
+
+
 def test_tsne_kernels_bit_exact(golden):
     g = golden("tsne_small.npz")
     import scipy.sparse as sp
