@@ -16,6 +16,10 @@ all host threads) timed on a bounded sample of the same workload (2 SGD epochs a
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n N]
     python bench.py --graph [--n N] [--steps K] [--warmup W] [--no-cpu-baseline]   (the fuzzy neighbour graph)
+
+transform / transform_plain: the served form (magnet_b200.serve) on a resident 200k x 64 layout: p50 / p99
+latency and points/s of transform() requests with Poisson arrivals at 200 per second, interleaved with fit
+requests, on 4 slots (continuous batching) and on 1 slot (one request at a time).
 """
 import argparse
 import json
@@ -443,6 +447,76 @@ def graph_bench(n, steps, warmup, cpu_baseline=True):
     print(json.dumps(out), flush=True)
 
 
+# ----------------------------------------------------------------------------------------------- served form
+def serve_workload(n=200_000, d=64, centers=50, seed=3):
+    """the served layout's data: a 50-Gaussian mixture in d = 64 (Dirichlet(1) weights, means N(0, 6^2), unit
+    covariance), seed 3; returns the rows and a sampler of new rows from the same mixture"""
+    rng = np.random.default_rng(seed)
+    wts = rng.dirichlet(np.ones(centers))
+    C = rng.normal(0, 6.0, (centers, d))
+
+    def draw(m, r):
+        return (C[r.choice(centers, m, p=wts)] + r.normal(0, 1, (m, d))).astype(np.float32)
+    return draw(n, rng), draw
+
+
+def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 50000), seed=3):
+    """The served form: a fitted 200k x 64 layout resident on the device; transform() requests of 1-4096 new rows
+    from the same mixture with Poisson arrivals at `rate` per second (100 SGD epochs each, the training rows
+    fixed), interleaved with fit requests of 5k-50k rows. Run once on one slot (the plain form: one request at a
+    time) and once on `slots` slots (continuous batching); latency is submit to result."""
+    from magnet_b200 import serve as S
+    import magnet_b200 as mg
+    t0 = time.perf_counter()
+    X, draw = serve_workload(seed=seed)
+    Y = S.fit_layout(X, n_epochs=200, seed=0)
+    a, b = mg.find_ab_params(1.0, 0.1)
+    layout = S.FittedLayout(X, Y, a=a, b=b, transform_epochs=100)
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(seed + 1)
+    sizes = rng.integers(1, 4097, n_requests)
+    gaps = rng.exponential(1.0 / rate, n_requests)
+    batches = [draw(int(m), rng) for m in sizes]
+    fit_at = dict(zip(sorted(rng.choice(np.arange(1, n_requests), len(fit_sizes), replace=False).tolist()),
+                      [draw(f, rng) for f in fit_sizes]))
+    big = batches[int(np.argmax(sizes))]
+
+    def run(k):
+        srv = S.device_server(layout, slots=k)
+        warm = [srv.submit("transform", (big, 0), layout.request_bytes(len(big)), len(big)) for _ in range(k)]
+        warm.append(srv.submit("fit", fit_at[min(fit_at)], S.fit_bytes(len(fit_at[min(fit_at)]), X.shape[1]), 0))
+        for f in warm:
+            f.result()
+        srv.done.clear()
+        futs = []
+        t_next = time.perf_counter()
+        for i in range(n_requests):
+            t_next += gaps[i]
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            m = int(sizes[i])
+            futs.append(srv.submit("transform", (batches[i], i), layout.request_bytes(m), m))
+            if i in fit_at:
+                Xf = fit_at[i]
+                futs.append(srv.submit("fit", Xf, S.fit_bytes(len(Xf), X.shape[1]), len(Xf)))
+        for f in futs:
+            f.result()
+        srv.close()
+        tr = S.latency_summary(srv.done, "transform")
+        fi = S.latency_summary(srv.done, "fit")
+        return {k2: round(v, 2) for k2, v in tr.items()}, {k2: round(v, 1) for k2, v in fi.items()}
+
+    plain, plain_fit = run(1)
+    mixed, mixed_fit = run(slots)
+    return {"transform": mixed | {"slots": slots}, "transform_plain": plain | {"slots": 1},
+            "fit_requests": {"mixed": mixed_fit, "plain": plain_fit},
+            "serve_config": {"layout": "200,000 x 64, 50-Gaussian mixture, seed 3, k=15, resident",
+                             "requests": n_requests, "rate_per_s": rate, "batch": "uniform integer [1, 4096]",
+                             "transform_epochs": 100, "fits": list(fit_sizes), "mode": "owner",
+                             "setup_s": round(setup_s, 1)}}
+
+
 # ----------------------------------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -453,6 +527,8 @@ def main():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graph", action="store_true", help="time the fuzzy neighbour graph instead of the layout")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--serve-requests", type=int, default=300)
     args = ap.parse_args()
     if args.graph:
         import torch
@@ -567,6 +643,11 @@ def main():
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
                                     "sample": "unavailable: %s" % e}
+    if not args.no_serve:
+        try:
+            line.update(serve_bench(n_requests=args.serve_requests))
+        except Exception as e:  # noqa: BLE001  (the layout's line is reported either way)
+            line["transform"] = {"error": "%s: %s" % (type(e).__name__, e)}
     if dist is not None:
         dist.destroy_process_group()
     if rank == 0:

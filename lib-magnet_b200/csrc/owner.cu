@@ -12,13 +12,14 @@
 //  2. schedule, one thread per edge: advances eons / eonns as the reference does and records each sampled edge's
 //     negatives count; then the chain pass, one warp per chunk: consumes the chunk's stream in edge order as
 //     the edge loop would (n_neg draws, the mid-range test and walk, the reverse-pull draws), recording at each
-//     head node the stream state where its edges start. It reads no position: the draws depend on positions only
-//     through a negative at distance 0 exactly (src/layout.cpp:181), which draws dim extra uniforms;
+//     head's first sampled edge the stream state where its draws start. It reads no position: the draws depend
+//     on positions only through a negative at distance 0 exactly (src/layout.cpp:181), which draws dim extra
+//     uniforms;
 //  3. node pass, one thread per head node: from its recorded state, replays the node's edges as the reference
 //     does (other positions from the snapshot, its own in registers) and writes its row. A negative at distance 0
 //     marks the node's chunk, since the states recorded after it are then off by dim draws;
-//  4. fallback, one thread per chunk, doing work for marked chunks only: restores the chunk's rows (and Adam
-//     state) from the snapshot and replays the whole chunk serially from the chunk's seed.
+//  4. fallback, one thread per chunk, doing work for marked chunks only: restores the rows of the chunk's heads
+//     (and their Adam state) from the snapshot and replays the whole chunk serially from the chunk's seed.
 // This file is compiled without FMA contraction (-fmad=false): every product and sum rounds on its own, as in
 // the reference's plain x86-64 build. The power kernel with b = rep_b = 1 under the sgd optimizer uses +, *, / and
 // sqrt only and reproduces the reference bit for bit; powf, expf, tanhf and coshf may differ from the host libm
@@ -282,9 +283,11 @@ __global__ void __launch_bounds__(256) owner_schedule_kernel(SgdDev c, OwnerDev 
 }
 
 // One warp per chunk: the chunk's stream consumed in edge order from the recorded negatives counts. The lanes
-// read 32 edges' counts at a time (coalesced) and take the sampled ones in order from a ballot; every lane holds
-// the same stream state and makes the same draws, so control flow stays uniform across the warp. No position is
-// read and nothing is stored but the per-node states.
+// read 32 edges' counts and heads at a time (coalesced) and take the sampled ones in order from a ballot; every
+// lane holds the same stream state and makes the same draws, so control flow stays uniform across the warp.
+// A head's state is recorded at its first sampled edge (edges that are not sampled draw nothing, and a head
+// without sampled edges draws nothing in the node pass), so heads without edges, such as the fixed training rows
+// of a transform, cost nothing. No position is read and nothing is stored but the per-node states.
 constexpr int kChainWarps = 4;   // chunks per block
 
 __global__ void __launch_bounds__(32 * kChainWarps) owner_chain_kernel(SgdDev c, OwnerDev o, int epoch,
@@ -295,28 +298,33 @@ __global__ void __launch_bounds__(32 * kChainWarps) owner_chain_kernel(SgdDev c,
     Rng r(stream_seed(c.seed, epoch, (uint64_t)k));
     const float inv_n_mid = c.n_mid > 0 ? 1.0f / (float)c.n_mid : 0.0f;
     const int32_t* __restrict__ rec = o.n_neg;
-    for (int64_t u = o.own[k]; u < o.own[k + 1]; ++u) {
-        if (lane == 0) o.node_state[u] = r.s;
-        // the reverse-pull rounds of each of u's edges: the same p for every edge of u
-        float p0 = 0.0f;
-        if (u >= c.n_fixed && mid_w > 0.0f && o.rev_indptr) {
-            const int32_t rs = o.rev_indptr[u], re = o.rev_indptr[u + 1];
-            if (re > rs) p0 = c.mid_rate * (float)(re - rs) * inv_n_mid;
-        }
-        const int64_t i0 = o.row[u], i1 = o.row[u + 1];
-        for (int64_t base = i0; base < i1; base += 32) {
-            const int64_t i = base + lane;
-            const int mine = i < i1 ? __ldg(rec + i) : kNotSampled;
-            unsigned todo = __ballot_sync(0xffffffffu, mine != kNotSampled);
-            while (todo) {
-                const int b = __ffs(todo) - 1;
-                todo &= todo - 1;
-                const int n_neg = __shfl_sync(0xffffffffu, mine, b);
-                for (int p = 0; p < n_neg; ++p) r.next();
-                if (mid_w > 0.0f && r.uniform() < c.mid_rate) (void)mid_partner(c, r, u, c.tail[base + b]);
-                for (float p = p0; p > 0.0f; p -= 1.0f)
-                    if (r.uniform() < p) (void)r.next();
+    const int64_t e0 = o.eown[k], e1 = o.eown[k + 1];
+    int64_t u = -1;
+    float p0 = 0.0f;
+    for (int64_t base = e0; base < e1; base += 32) {
+        const int64_t i = base + lane;
+        const int mine = i < e1 ? __ldg(rec + i) : kNotSampled;
+        const int32_t my_head = i < e1 ? c.head[i] : -1;
+        unsigned todo = __ballot_sync(0xffffffffu, mine != kNotSampled);
+        while (todo) {
+            const int b = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int n_neg = __shfl_sync(0xffffffffu, mine, b);
+            const int32_t h = __shfl_sync(0xffffffffu, my_head, b);
+            if (h != u) {
+                u = h;
+                if (lane == 0) o.node_state[u] = r.s;
+                // the reverse-pull rounds of each of u's edges: the same p for every edge of u
+                p0 = 0.0f;
+                if (u >= c.n_fixed && mid_w > 0.0f && o.rev_indptr) {
+                    const int32_t rs = o.rev_indptr[u], re = o.rev_indptr[u + 1];
+                    if (re > rs) p0 = c.mid_rate * (float)(re - rs) * inv_n_mid;
+                }
             }
+            for (int p = 0; p < n_neg; ++p) r.next();
+            if (mid_w > 0.0f && r.uniform() < c.mid_rate) (void)mid_partner(c, r, u, c.tail[base + b]);
+            for (float p = p0; p > 0.0f; p -= 1.0f)
+                if (r.uniform() < p) (void)r.next();
         }
     }
 }
@@ -344,7 +352,8 @@ __global__ void __launch_bounds__(32) owner_fallback_kernel(SgdDev c, OwnerDev o
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= o.n_chunks || !o.dirty[k]) return;
     o.dirty[k] = 0;
-    const int64_t u0 = o.own[k], u1 = o.own[k + 1];
+    // the heads of the chunk's edges (a marked chunk has at least one); rows without edges never move
+    const int64_t u0 = c.head[o.eown[k]], u1 = (int64_t)c.head[o.eown[k + 1] - 1] + 1;
     const int dim = c.dim;
     for (int64_t j = u0 * dim; j < u1 * dim; ++j) c.Y[j] = o.Yr[j];
     if (c.optimizer == 1) {
