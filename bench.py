@@ -460,6 +460,64 @@ def serve_workload(n=200_000, d=64, centers=50, seed=3):
     return draw(n, rng), draw
 
 
+def serve_stream(draw, n_requests, rate, fit_sizes, seed):
+    """the request stream of the served form: sizes uniform in [1, 4096], Poisson gaps at `rate`, the batches
+    and the fit requests' rows (submitted right after the transform request they are keyed by)"""
+    rng = np.random.default_rng(seed + 1)
+    sizes = rng.integers(1, 4097, n_requests)
+    gaps = rng.exponential(1.0 / rate, n_requests)
+    batches = [draw(int(m), rng) for m in sizes]
+    fit_at = dict(zip(sorted(rng.choice(np.arange(1, n_requests), len(fit_sizes), replace=False).tolist()),
+                      [draw(f, rng) for f in fit_sizes]))
+    return sizes, gaps, batches, fit_at
+
+
+def reference_serve(n_requests=300, rate=200.0, fit_sizes=(5000, 20000, 50000), seed=3, n_train=200_000):
+    """The served workload on the reference's CPU path (its compiled module on all host threads, driven as
+    MAGNET.fit / MAGNET.transform drive it): the same fitted 200k x 64 layout, built by the reference, and the
+    same request stream. The reference has no server, so requests run one at a time in arrival order: each starts
+    at max(its arrival, the previous request's end), with processing times measured."""
+    from oracle import oracle as O
+    if O.reference() is None:
+        return {"transform": {"unavailable": "the reference module (oracle/_ref) is not built"}}
+    t0 = time.perf_counter()
+    X, draw = serve_workload(n=n_train, seed=seed)
+    a, b = O.find_ab_params(1.0, 0.1)
+    Y, P = O.reference_fit(X, n_epochs=200, seed=0, a=a, b=b)
+    landmarks = O.choose_landmarks(n_train, 0)
+    step = O.transform_step(Y)
+    setup_s = time.perf_counter() - t0
+    sizes, gaps, batches, fit_at = serve_stream(draw, n_requests, rate, fit_sizes, seed)
+    arrivals = np.cumsum(gaps)
+    clock = 0.0
+    lat_t, lat_f = [], []
+    for i in range(n_requests):
+        start = max(arrivals[i], clock)
+        t = time.perf_counter()
+        O.reference_transform(X, P, Y, landmarks, step, batches[i], a=a, b=b, n_epochs=100, seed=i)
+        clock = start + (time.perf_counter() - t)
+        lat_t.append(clock - arrivals[i])
+        if i in fit_at:
+            start = max(arrivals[i], clock)
+            t = time.perf_counter()
+            O.reference_fit(fit_at[i], n_epochs=200, seed=0, a=a, b=b)
+            clock = start + (time.perf_counter() - t)
+            lat_f.append(clock - arrivals[i])
+    span = clock - arrivals[0]
+
+    def summary(lat, pts):
+        lat = np.asarray(lat) * 1e3
+        return {"requests": len(lat), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
+                "points_per_s": round(pts / max(span, 1e-9), 2)}
+    return {"transform": summary(lat_t, int(sizes.sum())) | {"slots": 1},
+            "fit_requests": summary(lat_f, int(sum(len(v) for v in fit_at.values()))),
+            "serve_config": {"layout": "200,000 x 64, 50-Gaussian mixture, seed 3, k=15 (built by the reference)",
+                             "requests": n_requests, "rate_per_s": rate, "batch": "uniform integer [1, 4096]",
+                             "transform_epochs": 100, "fits": list(fit_sizes), "cores": os.cpu_count(),
+                             "server": "one request at a time in arrival order", "setup_s": round(setup_s, 1)}}
+
+
 def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 50000), seed=3):
     """The served form: a fitted 200k x 64 layout resident on the device; transform() requests of 1-4096 new rows
     from the same mixture with Poisson arrivals at `rate` per second (100 SGD epochs each, the training rows
@@ -473,12 +531,7 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
     a, b = mg.find_ab_params(1.0, 0.1)
     layout = S.FittedLayout(X, Y, a=a, b=b, transform_epochs=100)
     setup_s = time.perf_counter() - t0
-    rng = np.random.default_rng(seed + 1)
-    sizes = rng.integers(1, 4097, n_requests)
-    gaps = rng.exponential(1.0 / rate, n_requests)
-    batches = [draw(int(m), rng) for m in sizes]
-    fit_at = dict(zip(sorted(rng.choice(np.arange(1, n_requests), len(fit_sizes), replace=False).tolist()),
-                      [draw(f, rng) for f in fit_sizes]))
+    sizes, gaps, batches, fit_at = serve_stream(draw, n_requests, rate, fit_sizes, seed)
     big = batches[int(np.argmax(sizes))]
 
     def run(k):
@@ -575,6 +628,11 @@ def main():
                 "cpu_baseline": {"value": round(value, 3), "unit": "s", "cores": nt, "kind": "reference",
                                  "sample": "per step: " + sample},
                 "e2e": {"value": round(value, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if not args.no_serve:
+            try:
+                line.update(reference_serve(n_requests=args.serve_requests))
+            except Exception as e:  # noqa: BLE001  (the layout's line is reported either way)
+                line["transform"] = {"error": "%s: %s" % (type(e).__name__, e)}
         if dist is not None:
             dist.destroy_process_group()
         print(json.dumps(line))

@@ -394,6 +394,108 @@ def optimize_sgd(Y, head, tail, eps, n_epochs, *, lr=1.0, mid_weight=0.0, mid_ph
     return Y
 
 
+def find_ab_params(spread=1.0, min_dist=0.1):
+    """magnet/__init__.py:26-48, the power kernel: a, b of 1 / (1 + a d^(2b)) fitted to the (min_dist, spread)
+    curve"""
+    from scipy.optimize import curve_fit
+    xv = np.linspace(0, spread * 3, 300)
+    yv = np.zeros(xv.shape)
+    yv[xv < min_dist] = 1.0
+    yv[xv >= min_dist] = np.exp(-(xv[xv >= min_dist] - min_dist) / spread)
+    params, _ = curve_fit(lambda x, a, b: 1.0 / (1.0 + a * x ** (2 * b)), xv, yv)
+    return float(params[0]), float(params[1])
+
+
+def reference_fuzzy_graph(ind, dist, n_neighbors, n_threads=-1):
+    """magnet/knn.py:215-230 on the compiled reference: its smooth_knn, then scipy's union"""
+    import scipy.sparse as sp
+    R = reference()
+    vals = np.asarray(R.smooth_knn(np.ascontiguousarray(dist, dtype=np.float32), int(n_neighbors), 1.0, 64,
+                                   int(n_threads)))
+    n, k = ind.shape
+    rows = np.repeat(np.arange(n, dtype=np.int64), k)
+    A = sp.csr_matrix((vals.ravel(), (rows, np.asarray(ind).ravel())), shape=(n, n), dtype=np.float32)
+    A.eliminate_zeros()
+    T = A.T.tocsr()
+    prod = A.multiply(T)
+    P = (1.0 * (A + T - prod) + 0.0 * prod).tocsr()
+    P.eliminate_zeros()
+    P.sort_indices()
+    return P
+
+
+def reference_fit(X, n_neighbors=15, n_epochs=200, seed=0, n_threads=-1, a=None, b=None, mid_weight=0.1):
+    """a fit on the reference's CPU path: its NN-descent kNN (magnet/knn.py:90-122), the fuzzy graph, the edge
+    schedule, a PCA start rescaled to max-abs 10 (the spectral init stays out of the timed path), its mid-near
+    pairs, and its SGD with the mid-range weight (MAGNET._optimize). Returns (Y, P)."""
+    R = reference()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n = X.shape[0]
+    k = min(n_neighbors, n) - 1
+    kin = min(max(k, 20), n - 1)
+    n_trees = int(max(2, min(8, round(np.sqrt(n) / 40))))
+    ind, d2 = R.nn_descent(X, int(kin), 50, 10, 0.001, n_trees, 30, int(seed), int(n_threads), False)
+    ind = np.asarray(ind)[:, :k].astype(np.int64)
+    dist = np.sqrt(np.maximum(np.asarray(d2)[:, :k], 0.0)).astype(np.float32)
+    P = reference_fuzzy_graph(ind, dist, n_neighbors, n_threads)
+    head, tail, eps = edge_schedule(P, n_epochs)
+    rng = np.random.default_rng(seed)
+    sub = X[rng.choice(n, min(n, 20000), replace=False)]
+    mu = sub.mean(0)
+    _, _, Vt = np.linalg.svd(sub - mu, full_matrices=False)
+    Y = ((X - mu) @ Vt[:2].T).astype(np.float32)
+    Y = np.ascontiguousarray(10.0 * Y / np.abs(Y).max(), dtype=np.float32)
+    pairs = np.asarray(R.mid_near_pairs_dense(X, 5, 6, int(seed), int(n_threads)))
+    if a is None or b is None:
+        a, b = find_ab_params(1.0, 0.1)
+    optimize_sgd(Y, head, tail, eps, n_epochs, mid_weight=mid_weight, mid_pairs=pairs, backend="reference",
+                 n_threads=n_threads, seed=seed, a=a, b=b, indptr=P.indptr, indices=P.indices)
+    return Y, P
+
+
+def choose_landmarks(n, random_state=0):
+    """magnet/knn.py:125-128"""
+    m = int(min(n, max(100, 4 * np.sqrt(n))))
+    return np.sort(np.random.default_rng(random_state).choice(n, m, replace=False)).astype(np.int32)
+
+
+def transform_step(Y_train):
+    """the transform step scale of magnet/__init__.py:899-906: min(1, median 1-NN spacing / 0.14)"""
+    from sklearn.neighbors import NearestNeighbors
+    n = Y_train.shape[0]
+    sub = Y_train[np.random.default_rng(0).choice(n, min(n, 5000), replace=False)]
+    d1 = float(np.median(NearestNeighbors(n_neighbors=2).fit(Y_train).kneighbors(sub)[0][:, 1]))
+    return float(min(1.0, d1 / 0.14))
+
+
+def reference_transform(X_train, P, Y_train, landmarks, step, Q, *, a, b, n_neighbors=15, n_epochs=100, seed=0,
+                        n_threads=-1):
+    """MAGNET.transform (magnet/__init__.py:876-930) on the reference's CPU path: its beam search over the
+    training graph (knn_search, magnet/knn.py:131-152), smooth_knn, the start at the membership-weighted mean,
+    the schedule, and its SGD with the training rows fixed at the spacing-scaled step"""
+    R = reference()
+    n_train = Y_train.shape[0]
+    k = min(n_neighbors, n_train) - 1
+    Q = np.ascontiguousarray(Q, dtype=np.float32)
+    ind, d2 = R.knn_search(X_train, P.indptr.astype(np.int32), P.indices.astype(np.int32), landmarks, Q, int(k),
+                           int(max(64, 2 * k + 10)), 5, int(seed), int(n_threads))
+    ind = np.asarray(ind).astype(np.int64)
+    dist = np.sqrt(np.maximum(np.asarray(d2), 0.0)).astype(np.float32)
+    vals = np.asarray(R.smooth_knn(dist, int(n_neighbors), 1.0, 64, int(n_threads)))
+    W = vals / np.maximum(vals.sum(1, keepdims=True), 1e-12)
+    Y_new = np.einsum("mk,mkd->md", W, Y_train[ind]).astype(np.float32)
+    m = Q.shape[0]
+    Y_all = np.ascontiguousarray(np.vstack([Y_train, Y_new]), dtype=np.float32)
+    freq = sampling_frequencies(vals.ravel().astype(np.float64), 5.0 * m)
+    keep = freq >= 1.0 / n_epochs
+    head = (n_train + np.repeat(np.arange(m), k)).astype(np.int32)[keep]
+    tail = ind.ravel().astype(np.int32)[keep]
+    eps = (1.0 / freq[keep]).astype(np.float32)
+    optimize_sgd(Y_all, head, tail, eps, n_epochs, lr=step, backend="reference", n_threads=n_threads, seed=seed,
+                 a=a, b=b, n_fixed=n_train)
+    return Y_all[n_train:]
+
+
 def optimize_tsne(P, Y, n_iter=750, early_iter=250, early_exaggeration=12.0, exaggeration=1.0,
                   learning_rate=None, momentum=(0.5, 0.8), n_interp=3, box_width=0.7, n_threads=-1,
                   dof=1.0, backend="reference", callback=None):
