@@ -165,6 +165,10 @@ typedef struct {
     /* owner mode: who chose each node as a mid-range partner, CSR (n + 1, rev_nnz), or NULL
        (rev_indptr / rev_indices of src/bindings.cpp:23) */
     const int32_t* rev_indptr; const int32_t* rev_indices; int64_t rev_nnz;
+    /* owner mode: edges per chunk; 0 = the reference's 4096 (src/layout.cpp:448). Smaller chunks give more
+       independent streams (a deterministic result of its own, not the reference's owner stream assignment);
+       the server uses them for small transforms. */
+    int owner_chunk_edges;
 } mg_layout_args;
 
 /* Fills a with the reference's defaults for the scalars (pointers NULL). */

@@ -463,6 +463,7 @@ SgdDev prepare_sgd(const mg_layout_args& A, cudaStream_t s) {
     require(A.loss == 0 || A.kernel == 0, "the InfoNCE loss supports the power kernel only");
     require(A.parallel == 0 || A.parallel == 1, "parallel must be 0 (hogwild) or 1 (owner)");
     require(A.parallel == 0 || A.loss == 0, "parallel='owner' supports the umap loss only (InfoNCE moves the negatives)");
+    require(A.owner_chunk_edges >= 0, "owner_chunk_edges must be 0 (the reference's chunks) or positive");
     require(A.n_fixed >= 0 && A.n_fixed <= n, "n_fixed out of range");
     require(A.stream_mode == 0 || A.stream_mode == 1, "stream_mode must be 0 (per-edge streams) or 1 (serial stream)");
     if (A.parallel == 0 && A.stream_mode == 1 && A.optimizer == 1)
@@ -592,8 +593,8 @@ extern "C" int mg_optimize_layout(const mg_layout_args* a) {
             const int32_t* rp = a->rev_indptr ? in_dev(a->rev_indptr, c.n + 1, 21, s) : nullptr;
             const int32_t* rx = a->rev_indptr ? in_dev(a->rev_indices, a->rev_nnz, 22, s) : nullptr;
             if (c.n_edges > 0 && a->epoch_end > a->epoch_start)
-                owner_run(c, *g_sgd_work, rp, rx, a->epoch_start, a->epoch_end, a->alpha0, a->alpha1, a->mid_w0,
-                          a->mid_w1, s);
+                owner_run(c, *g_sgd_work, rp, rx, a->owner_chunk_edges, a->epoch_start, a->epoch_end, a->alpha0,
+                          a->alpha1, a->mid_w0, a->mid_w1, s);
         } else if (c.n_edges > 0 && a->epoch_end > a->epoch_start) {
             sgd_run(c, *g_sgd_work, a->stream_mode, a->epoch_start, a->epoch_end, a->alpha0, a->alpha1, a->mid_w0,
                     a->mid_w1, s);

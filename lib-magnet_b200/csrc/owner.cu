@@ -375,8 +375,9 @@ void owner_epoch_launch(const SgdDev& c, const OwnerDev& o, int epoch, float alp
 
 }  // namespace
 
-int owner_chunk_count(int64_t n_edges) {
-    return (int)std::min<int64_t>(4096, std::max<int64_t>(1, n_edges / 4096));
+int owner_chunk_count(int64_t n_edges, int chunk_edges) {
+    const int64_t per = chunk_edges > 0 ? chunk_edges : 4096;
+    return (int)std::min<int64_t>(chunk_edges > 0 ? INT32_MAX / 2 : 4096, std::max<int64_t>(1, n_edges / per));
 }
 
 bool owner_heads_sorted(const int32_t* head_dev, int64_t n_edges, SgdWork& w, cudaStream_t s) {
@@ -391,11 +392,11 @@ bool owner_heads_sorted(const int32_t* head_dev, int64_t n_edges, SgdWork& w, cu
     return h == 0;
 }
 
-void owner_run(SgdDev& c, SgdWork& w, const int32_t* rev_indptr, const int32_t* rev_indices, int e0, int e1,
-               float alpha0, float alpha1, float mid_w0, float mid_w1, cudaStream_t s) {
+void owner_run(SgdDev& c, SgdWork& w, const int32_t* rev_indptr, const int32_t* rev_indices, int chunk_edges,
+               int e0, int e1, float alpha0, float alpha1, float mid_w0, float mid_w1, cudaStream_t s) {
     const int64_t n = c.n, E = c.n_edges;
     const int dim = c.dim;
-    const int nc = owner_chunk_count(E);
+    const int nc = owner_chunk_count(E, chunk_edges);
     OwnerDev o{};
     int64_t* row = static_cast<int64_t*>(w.o_row.ensure(sizeof(int64_t) * (n + 1)));
     int64_t* own = static_cast<int64_t*>(w.o_own.ensure(sizeof(int64_t) * (nc + 1) * 2));

@@ -48,11 +48,12 @@ void sgd_record(SgdDev& c, SgdWork& w, int stream_mode, int epoch, float alpha, 
                 int64_t* off_out, int32_t* negs, int64_t negs_cap, int32_t* mid, int64_t* n_negs_dev,
                 cudaStream_t s);
 
-// owner mode (parallel = 1, src/layout.cpp:441-463): chunk count for E edges, the sorted-heads check (device
-// heads; synchronises s), and epochs [e0, e1); the reverse mid pairs are device arrays or NULL
-int owner_chunk_count(int64_t n_edges);
+// owner mode (parallel = 1, src/layout.cpp:441-463): chunk count for E edges (chunk_edges 0: the reference's
+// min(4096, max(1, E / 4096)); else max(1, E / chunk_edges)), the sorted-heads check (device heads; synchronises
+// s), and epochs [e0, e1); the reverse mid pairs are device arrays or NULL
+int owner_chunk_count(int64_t n_edges, int chunk_edges);
 bool owner_heads_sorted(const int32_t* head_dev, int64_t n_edges, SgdWork& w, cudaStream_t s);
-void owner_run(SgdDev& c, SgdWork& w, const int32_t* rev_indptr, const int32_t* rev_indices, int e0, int e1,
-               float alpha0, float alpha1, float mid_w0, float mid_w1, cudaStream_t s);
+void owner_run(SgdDev& c, SgdWork& w, const int32_t* rev_indptr, const int32_t* rev_indices, int chunk_edges,
+               int e0, int e1, float alpha0, float alpha1, float mid_w0, float mid_w1, cudaStream_t s);
 
 }  // namespace mgb

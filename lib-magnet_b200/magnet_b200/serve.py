@@ -13,7 +13,11 @@ slots and device memory free up, and their work overlaps on the device.
   set), smooth_knn memberships (device), the start at the membership-weighted mean of the neighbours' positions,
   the reference's edge schedule and step scale, then the SGD with the training rows fixed (n_fixed), on the
   device. Owner mode (parallel='owner', the default here) makes a request's result a function of its inputs
-  alone, so it is the same bits alone and in any mix; parallel='hogwild' agrees to float rounding.
+  alone, so it is the same bits alone and in any mix; parallel='hogwild' agrees to float rounding. The owner
+  chunks are 256 edges (owner_chunk_edges) instead of the reference's 4096: a transform has few edges, and
+  each chunk is one serial stream, so smaller chunks run more streams side by side. The result is
+  deterministic but does not reproduce the reference's owner-mode streams. The reference's own transform runs
+  hogwild, which has no reproducible streams either.
 * ``fit_layout``: a fit request (exact kNN, fuzzy graph, edge schedule, PCA start, SGD), on the device.
 
 Each worker thread owns a CUDA stream: torch work runs on it and the C ABI is pointed at it (mg_set_stream is
@@ -153,7 +157,8 @@ class FittedLayout:
     """A fitted layout resident on the device: training rows X (n, d), layout Y (n, 2), kernel constants."""
 
     def __init__(self, X, Y, *, a, b, rep_a=None, rep_b=1.0, n_neighbors=15, transform_epochs=100,
-                 learning_rate=1.0, samples_per_node=5.0, parallel="owner", seed=0, query_block=1024):
+                 learning_rate=1.0, samples_per_node=5.0, parallel="owner", seed=0, query_block=1024,
+                 owner_chunk_edges=256):
         import torch
         self.torch = torch
         self.dev = torch.device("cuda", torch.cuda.current_device())
@@ -173,6 +178,12 @@ class FittedLayout:
         self.parallel = {"owner": 1, "hogwild": 0}[parallel]
         self.seed = int(seed)
         self.block = int(query_block)
+        self.chunk_edges = int(owner_chunk_edges)
+        # column tiles of the two-stage top-k: a divisor of n in [1024, 8192] when there is one, else 4096 with
+        # the last tile padded
+        divisors = [t for t in range(8192, 1023, -1) if self.n % t == 0]
+        self.tile = divisors[0] if divisors else min(4096, self.n)
+        self.n_tiles = -(-self.n // self.tile)
         # the step in units of the layout's own spacing (magnet/__init__.py:899-906): min(1, median 1-NN / 0.14)
         from scipy.spatial import cKDTree
         sub = Y[np.random.default_rng(0).choice(self.n, min(self.n, 5000), replace=False)]
@@ -194,18 +205,29 @@ class FittedLayout:
         return st
 
     def knn(self, Qd):
-        """exact k nearest training rows of the query rows (squared euclidean), sorted: (ind, dist) on the device"""
+        """exact k nearest training rows of the query rows (squared euclidean), sorted: (ind, dist) on the device.
+        The top-k runs in two stages: the k smallest of every tile of `tile` columns, then the k smallest of those
+        candidates; a tile's top-k over a few thousand columns is far cheaper than one over all n."""
         torch = self.torch
         m = Qd.shape[0]
         qs = (Qd * Qd).sum(1)
         ind = torch.empty((m, self.k), dtype=torch.int64, device=self.dev)
         dist = torch.empty((m, self.k), dtype=torch.float32, device=self.dev)
+        T, nt = self.tile, self.n_tiles
         for s in range(0, m, self.block):
             q = Qd[s:s + self.block]
-            d2 = qs[s:s + self.block, None] - 2.0 * (q @ self.Xd.T) + self.sq[None, :]
-            v, i = torch.topk(d2, self.k, dim=1, largest=False, sorted=True)
-            ind[s:s + q.shape[0]] = i
-            dist[s:s + q.shape[0]] = torch.sqrt(torch.clamp(v, min=0.0))
+            r = q.shape[0]
+            # |x|^2 - 2 q.x in one GEMM with bias; the row's |q|^2 does not change its order and is added to the
+            # k selected values only
+            d2 = torch.addmm(self.sq[None, :].expand(r, self.n), q, self.Xd.T, beta=1.0, alpha=-2.0)
+            if nt * T != self.n:
+                d2 = torch.cat([d2, torch.full((r, nt * T - self.n), float("inf"), device=self.dev)], 1)
+            v1, i1 = torch.topk(d2.view(r, nt, T), self.k, dim=2, largest=False, sorted=False)
+            v, j = torch.topk(v1.reshape(r, nt * self.k), self.k, dim=1, largest=False, sorted=True)
+            tile_of = torch.div(j, self.k, rounding_mode="floor")
+            local = torch.gather(i1.reshape(r, nt * self.k), 1, j)
+            ind[s:s + r] = tile_of * T + local
+            dist[s:s + r] = torch.sqrt(torch.clamp(v + qs[s:s + r, None], min=0.0))
         return ind, dist
 
     def transform(self, X_new, seed=None):
@@ -242,7 +264,7 @@ class FittedLayout:
             N.optimize_layout(Y_all, head, tail, eps, eons, eonns, z, z, 0, self.epochs, self.lr, 0.0, 0.0, 0.0,
                               self.a, self.b, self.rep_a, self.rep_b, 5.0, 0, 1.0, 2.0, 4, 0.25, 0, 0, self.n,
                               z2, z2, z, 0.9, 0.999, z, np.zeros((0, 1), np.int32), z, z, 0.0, 0, zf, sd, -1,
-                              self.parallel, None, None, 0)
+                              self.parallel, None, None, 0, owner_chunk_edges=self.chunk_edges)
             out = Y_all[self.n:].cpu().numpy()
         return out
 

@@ -136,7 +136,7 @@ void optimize_layout(py::object Y, py::object head, py::object tail, py::object 
                      py::object adam_v, py::object adam_t, float beta1, float beta2, py::object walk_lens,
                      py::object mid_pairs, py::object jump_indptr, py::object jump_indices, float mid_jump, int kernel,
                      py::object node_b, uint64_t seed, int n_threads, int parallel, py::object rev_indptr,
-                     py::object rev_indices, int stream_mode) {
+                     py::object rev_indices, int stream_mode, int owner_chunk_edges) {
     auto y = view<float>(Y);
     if (y.ndim() != 2) throw std::runtime_error("Y must be 2-dimensional");
     auto h = view<int32_t>(head), t = view<int32_t>(tail);
@@ -182,7 +182,7 @@ void optimize_layout(py::object Y, py::object head, py::object tail, py::object 
     A.jump_indptr = jp.size() > 0 ? jp.ptr : nullptr; A.jump_indices = jx.size() > 0 ? jx.ptr : nullptr;
     A.jump_nnz = jx.size(); A.mid_jump = mid_jump;
     A.kernel = kernel; A.node_b = nb.size() > 0 ? nb.ptr : nullptr; A.seed = seed; A.n_threads = n_threads;
-    A.parallel = parallel; A.stream_mode = stream_mode;
+    A.parallel = parallel; A.stream_mode = stream_mode; A.owner_chunk_edges = owner_chunk_edges;
     if (parallel == 1 && rp.size() > 0) {
         A.rev_indptr = rp.ptr; A.rev_indices = rx.size() > 0 ? rx.ptr : nullptr; A.rev_nnz = rx.size();
     }
@@ -289,7 +289,7 @@ PYBIND11_MODULE(_native, m) {
           py::arg("walk_lens"), py::arg("mid_pairs"), py::arg("jump_indptr"), py::arg("jump_indices"),
           py::arg("mid_jump"), py::arg("kernel"), py::arg("node_b"), py::arg("seed"), py::arg("n_threads"),
           py::arg("parallel") = 0, py::arg("rev_indptr") = py::none(), py::arg("rev_indices") = py::none(),
-          py::arg("stream_mode") = 0);
+          py::arg("stream_mode") = 0, py::arg("owner_chunk_edges") = 0);
     m.def("layout_schedule", &layout_schedule, "draws of one SGD epoch (test hook): (sampled, n_neg, neg_off, negs, mid)",
           py::arg("Y"), py::arg("head"), py::arg("tail"), py::arg("epochs_per_sample"), py::arg("epoch_of_next_sample"),
           py::arg("epoch_of_next_negative_sample"), py::arg("epoch"), py::arg("epoch_start"), py::arg("epoch_end"),
