@@ -234,7 +234,11 @@ class FittedLayout:
         """new rows (m, d) -> their layout positions (m, 2), on this thread's stream"""
         torch = self.torch
         from . import _native as N
-        st = getattr(_THREAD, "stream", None) or self.bind_stream()
+        st = getattr(_THREAD, "stream", None)
+        if st is None:
+            # a thread that is not a server worker: the caller's current stream, for torch and the C ABI alike
+            st = torch.cuda.current_stream(self.dev)
+            _lib().mg_set_stream(ctypes.c_void_p(st.cuda_stream))
         with torch.cuda.stream(st):
             Q = torch.from_numpy(np.ascontiguousarray(X_new, dtype=np.float32)).to(self.dev, non_blocking=False)
             m = Q.shape[0]

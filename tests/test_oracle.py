@@ -180,3 +180,40 @@ def test_schedule_record_matches_serial_run(golden):
         assert negs.size == n_neg.sum()
         assert ((negs >= 0) & (negs < g["Y0"].shape[0])).all()
     assert np.array_equal(eons, g["eons_default"]) and np.array_equal(eonns, g["eonns_default"])
+
+
+def test_reference_fit_and_transform_glue(ref):
+    """the reference arm's served path on the compiled reference: a fit (NN-descent, fuzzy graph, schedule, mid
+    pairs, SGD) and MAGNET.transform (beam-search kNN, memberships, fixed-row SGD) place new rows in their blob"""
+    if ref is None:
+        pytest.skip("reference module not built")
+    from sklearn.neighbors import KNeighborsClassifier
+    a, b = O.find_ab_params(1.0, 0.1)
+    assert abs(a - 1.577) < 2e-3 and abs(b - 0.895) < 2e-3
+    rng = np.random.default_rng(1)
+    C = rng.normal(0, 6, (6, 16))
+    y = rng.integers(0, 6, 3000)
+    X = (C[y] + rng.normal(0, 1, (3000, 16))).astype(np.float32)
+    Y, P = O.reference_fit(X[:2500], n_epochs=60, seed=0, a=a, b=b)
+    assert Y.shape == (2500, 2) and np.isfinite(Y).all() and P.shape == (2500, 2500)
+    Yn = O.reference_transform(X[:2500], P, Y, O.choose_landmarks(2500), O.transform_step(Y), X[2500:], a=a, b=b,
+                               n_epochs=50, seed=1)
+    assert Yn.shape == (500, 2) and np.isfinite(Yn).all()
+    assert KNeighborsClassifier(10).fit(Y, y[:2500]).score(Yn, y[2500:]) > 0.9
+
+
+def test_served_request_stream_is_seeded():
+    """both arms of the served measurement draw the same stream: sizes in [1, 4096], Poisson gaps, fit requests
+    keyed by the transform request they follow"""
+    import bench as B
+    rng = np.random.default_rng(0)
+    C = rng.normal(0, 6, (3, 4))
+
+    def draw(m, r):
+        return (C[r.integers(0, 3, m)] + r.normal(0, 1, (m, 4))).astype(np.float32)
+    s1 = B.serve_stream(draw, 40, 200.0, (50, 80), 3)
+    s2 = B.serve_stream(draw, 40, 200.0, (50, 80), 3)
+    assert np.array_equal(s1[0], s2[0]) and np.array_equal(s1[1], s2[1])
+    assert all(np.array_equal(x, z) for x, z in zip(s1[2], s2[2]))
+    assert s1[0].min() >= 1 and s1[0].max() <= 4096 and (s1[1] > 0).all()
+    assert sorted(len(v) for v in s1[3].values()) == [50, 80] and all(0 < k < 40 for k in s1[3])
