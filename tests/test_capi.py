@@ -20,7 +20,8 @@ def declared():
 def test_header_declares_entry_points():
     names = declared()
     for must in ("mg_fftconv_create", "mg_fftconv_compute", "mg_optimize_layout", "mg_optimize_tsne",
-                 "mg_tsne_attraction", "mg_tsne_step", "mg_bbox_2d", "mg_last_error"):
+                 "mg_tsne_attraction", "mg_tsne_step", "mg_bbox_2d", "mg_last_error", "mg_smooth_knn",
+                 "mg_fuzzy_union"):
         assert must in names
 
 
@@ -43,10 +44,28 @@ def test_error_convention_without_gpu():
     assert rc == 1 and b"5-smooth" in lib.mg_last_error()
 
 
+def test_graph_argument_errors_without_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(LIB)
+    lib.mg_last_error.restype = ctypes.c_char_p
+    P, I64 = ctypes.c_void_p, ctypes.c_int64
+    lib.mg_fuzzy_union.argtypes = [P, P, I64, ctypes.c_int, I64, ctypes.c_double, P, P, P, I64, ctypes.POINTER(I64)]
+    lib.mg_smooth_knn.argtypes = [P, I64, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, P]
+    nnz = I64(0)
+    buf = (ctypes.c_int32 * 8)()
+    # a graph of 4 nodes cannot hold 6 kNN rows
+    rc = lib.mg_fuzzy_union(buf, buf, 6, 1, 4, 1.0, buf, buf, buf, 8, ctypes.byref(nnz))
+    assert rc == 1 and b"n_rows <= n" in lib.mg_last_error()
+    rc = lib.mg_smooth_knn(buf, 2, 2, 0, 1.0, 64, buf)
+    assert rc == 1 and b"n_neighbors must be positive" in lib.mg_last_error()
+
+
 def test_native_surface_has_reference_names():
     mod = pytest.importorskip("magnet_b200._native")
     for name in ("FFTConv2D", "optimize_layout", "tsne_attraction", "tsne_step", "tsne_update", "bbox_2d",
-                 "mid_spring"):
+                 "mid_spring", "smooth_knn", "fuzzy_union"):
         assert hasattr(mod, name)
     import _magnet
     assert _magnet.optimize_layout is mod.optimize_layout
+    assert _magnet.smooth_knn is mod.smooth_knn
