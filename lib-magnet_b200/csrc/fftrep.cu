@@ -483,7 +483,7 @@ void rep_gather_forces(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, f
 }
 
 void ensure_fft_attrs() {
-    static int done_dev = -1;
+    static thread_local int done_dev = -1;   // per thread: host threads may drive layouts side by side
     int dev = 0;
     MGB_CUDA(cudaGetDevice(&dev));
     if (done_dev == dev) return;

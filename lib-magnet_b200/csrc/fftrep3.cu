@@ -348,7 +348,8 @@ void fft3_build_plans(DevBuf& table, int Mmax, int& Mp_max) {
 
 // resident blocks of the column kernel for this buffer size (raises its shared-memory limit once per device)
 int col3_blocks(int Mp_max) {
-    static int cached_dev = -1, cached_mp = -1, cached_blocks = 0;
+    // per thread: host threads may drive layouts side by side
+    static thread_local int cached_dev = -1, cached_mp = -1, cached_blocks = 0;
     int dev = 0, optin = 0;
     MGB_CUDA(cudaGetDevice(&dev));
     if (cached_dev == dev && cached_mp == Mp_max) return cached_blocks;
@@ -384,7 +385,8 @@ int row3_blocks(const void* fn, int Mp_max) {
 namespace {
 struct RowBlocks {
     int dev = -1, mp = -1, fwd = 0, inv = 0;
-} g_row_blocks;
+};
+thread_local RowBlocks g_row_blocks;   // per thread, as the column cache
 }  // namespace
 
 // launch sizes of the row kernels (and their shared-memory limits) for this device and buffer size; called when

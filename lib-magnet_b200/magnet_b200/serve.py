@@ -191,10 +191,14 @@ class FittedLayout:
         self.lr = float(learning_rate) * float(min(1.0, d1 / 0.14))
 
     def request_bytes(self, m):
-        """device bytes a transform of m rows holds at its peak: a block of query distances, the neighbour
-        arrays, the layout copy and the SGD's per-edge and per-node scratch"""
+        """device bytes a transform of m rows holds at its peak: a block of query distances (and its padded copy
+        when the tiles do not divide n), the first-stage top-k candidates, the neighbour arrays, the layout copy
+        and the SGD's per-edge and per-node scratch"""
         mb = min(m, self.block)
-        return 4 * mb * self.n + 64 * m * self.k + 48 * (self.n + m)
+        padded = self.n_tiles * self.tile
+        dist_block = 4 * mb * self.n + (4 * mb * padded if padded != self.n else 0)
+        candidates = 12 * mb * self.n_tiles * self.k
+        return dist_block + candidates + 64 * m * self.k + 48 * (self.n + m)
 
     def bind_stream(self, slot=None):
         """give this thread a CUDA stream of its own: torch's current stream for the thread, and the C ABI's"""
