@@ -111,9 +111,9 @@ def expected(g, opts, name):
 # the start of the epoch. The "_b1" cases use only +, *, / and sqrt (power kernel with b = rep_b = 1, the sgd
 # optimizer), which the device evaluates as the reference's plain x86-64 build does; the others go through powf,
 # expf or tanhf. "large" is an 8000-node graph (23 chunks); "dup" starts from 16 distinct positions, so that
-# negatives at distance 0 draw the jitter.
+# negatives at distance 0 draw the jitter (with Adam, the replay also restores the Adam state).
 OWNER_CASES = ["b1_pairs", "b1_walk_fixed", "b1_jump_norm_dim3", "b1_dim8", "b1_large", "b1_dup", "pairs",
-               "adam_b1", "node_b", "gaussian_large"]
+               "adam_b1", "adam_b1_dup", "node_b", "gaussian_large"]
 
 
 def synthetic_graph(n=8000, k=12, centers=8, seed=3):
@@ -152,12 +152,12 @@ def owner_state(g, name, seed=12345, big=None):
     n = g["Y0"].shape[0]
     dim = {"b1_jump_norm_dim3": 3, "b1_dim8": 8}.get(name, 2)
     Y = _initial(g, dim)
-    if name == "b1_dup":
+    if name.endswith("_dup"):
         Y = np.random.default_rng(4).uniform(-10, 10, (16, 2)).astype(np.float32)[np.arange(n) % 16]
     kw = _base_kw(g, dim, seed)
-    if name.startswith("b1") or name == "adam_b1":
+    if name.startswith("b1") or name.startswith("adam_b1"):
         kw.update(b=1.0, rep_a=1.7, rep_b=1.0)
-    if name == "adam_b1":
+    if name.startswith("adam_b1"):
         _adam_state(kw, n, dim)
     elif name == "b1_walk_fixed":
         kw.update(indptr=g["indptr"], indices=g["indices"], mid_pairs=np.zeros((0, 1), np.int32), n_fixed=100)
