@@ -69,3 +69,26 @@ def test_native_surface_has_reference_names():
     import _magnet
     assert _magnet.optimize_layout is mod.optimize_layout
     assert _magnet.smooth_knn is mod.smooth_knn
+
+
+def test_owner_mode_argument_rules_without_gpu(golden):
+    """owner mode's argument rules (src/layout.cpp:375-377, 441-446) and the reverse-pull bound are checked on
+    the host before any device work"""
+    pytest.importorskip("magnet_b200._native")
+    import numpy as np
+    import magnet_b200 as mg
+    import sgd_cases as C
+    g = golden("sgd_small.npz")
+    gg, Y, eons, eonns, kw, rp, rx = C.owner_state(g, "b1_pairs")
+    args = (Y, gg["head"], gg["tail"], gg["eps"], eons, eonns)
+    with pytest.raises(RuntimeError, match="supports the umap loss only"):
+        mg.optimize_layout(*args, n_threads=1, parallel=1, **(kw | dict(loss=1)))
+    head = gg["head"].copy()
+    head[[10, 500]] = head[[500, 10]]
+    with pytest.raises(RuntimeError, match="needs edges sorted by head"):
+        mg.optimize_layout(Y, head, *args[2:], n_threads=1, parallel=1, **kw)
+    with pytest.raises(RuntimeError, match="at most 65536"):
+        mg.optimize_layout(*args, n_threads=1, parallel=1, rev_indptr=rp, rev_indices=rx, **(kw | dict(mid_rate=1e9)))
+    with pytest.raises(RuntimeError, match="owner_chunk_edges"):
+        mg.optimize_layout(*args, n_threads=1, parallel=1, owner_chunk_edges=-1, **kw)
+    assert np.array_equal(Y, C.owner_state(g, "b1_pairs")[1])
