@@ -6,7 +6,7 @@ by the reference's own code: its compiled `_magnet` (optimize_layout at n_thread
 tsne_attraction, tsne_step, bbox_2d, smooth_knn) and its Python drivers (magnet/tsne.py FFTRepulsion2D /
 optimize_tsne, magnet/knn.py fuzzy_graph, magnet/__init__.py edge schedule). Inputs are seeded synthetic data.
 
-    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner graph]
+    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner graph tsne_variants]
 """
 import os
 import sys
@@ -200,6 +200,19 @@ def graph_fixture():
     np.savez_compressed(os.path.join(HERE, "graph_small.npz"), **out)
 
 
+def tsne_variants_fixture():
+    """the reference's optimize_tsne (magnet/tsne.py) on tsne_small.npz's graph and start, 60 iterations (20 early),
+    with options other than the defaults: heavy tails (dof 0.7), 5 interpolation points per box over wider boxes,
+    and late exaggeration with a higher late momentum"""
+    g = dict(np.load(os.path.join(HERE, "tsne_small.npz")))
+    P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]))
+    from tsne_cases import TSNE_VARIANTS
+    out = {}
+    for name, kw in TSNE_VARIANTS.items():
+        out["Y_" + name] = optimize_tsne(P, g["Y0"].copy(), n_iter=60, early_iter=20, n_threads=1, **kw)
+    np.savez_compressed(os.path.join(HERE, "tsne_variants.npz"), **out)
+
+
 def sgd_owner_fixture():
     """the reference's owner mode (parallel=1, 4 threads; its result does not depend on the thread count) on each
     owner case of sgd_cases.py: the final Y and sha-256 digests of eons, eonns and the Adam state at seed 12345,
@@ -226,10 +239,10 @@ def sgd_owner_fixture():
 
 if __name__ == "__main__":
     # all fixtures, or only those named on the command line (sgd_options reads sgd_small.npz)
-    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner", "graph"]
+    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner", "graph", "tsne_variants"]
     for name in todo:
         {"sgd": sgd_fixture, "fft": fft_fixture, "tsne": tsne_fixture, "sgd_options": sgd_options_fixture,
-         "sgd_owner": sgd_owner_fixture, "graph": graph_fixture}[name]()
+         "sgd_owner": sgd_owner_fixture, "graph": graph_fixture, "tsne_variants": tsne_variants_fixture}[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

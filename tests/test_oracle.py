@@ -137,6 +137,20 @@ def test_tsne_driver_restatement(golden):
     assert np.array_equal(Y, g["Y_tsne60"])
 
 
+def test_tsne_driver_variants(golden, ref):
+    """the restated driver reproduces the reference's optimize_tsne bit for bit away from the defaults too (heavy
+    tails, 5 interpolation points over wider boxes, late exaggeration and momentum; tsne_variants.npz)"""
+    from tsne_cases import TSNE_VARIANTS
+    if ref is None:
+        pytest.skip("reference module not built")
+    import scipy.sparse as sp
+    g, v = golden("tsne_small.npz"), golden("tsne_variants.npz")
+    P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]))
+    for name, kw in TSNE_VARIANTS.items():
+        Y = O.optimize_tsne(P, g["Y0"].copy(), n_iter=60, early_iter=20, n_threads=1, backend="reference", **kw)
+        assert np.array_equal(Y, v["Y_" + name]), name
+
+
 @pytest.mark.parametrize("ni", [5, 3])
 def test_grid_and_spectra_restatement(golden, ni):
     g = golden("fft_small.npz")
