@@ -76,6 +76,22 @@ def test_device_loop_against_reference_driver(mg, golden, use_graph):
     assert abs(knn_overlap(g["X"], Y) - knn_overlap(g["X"], Yr)) < 0.02
 
 
+@pytest.mark.parametrize("name", ["dof07", "interp5", "exag"])
+def test_device_loop_variants_against_reference_driver(mg, golden, name):
+    """the device loop away from the defaults (heavy tails, 5 interpolation points over wider boxes, late
+    exaggeration and momentum) against the reference's own optimize_tsne on the same graph and start: KL within
+    1 % and 15-NN overlap within 0.02"""
+    from tsne_cases import TSNE_VARIANTS
+    g, v = golden("tsne_small.npz"), golden("tsne_variants.npz")
+    P, Pn = normed(g)
+    Y = mg.optimize_tsne(P, g["Y0"].copy(), n_iter=60, early_iter=20, **TSNE_VARIANTS[name])
+    Yr = v["Y_" + name]
+    assert np.isfinite(Y).all()
+    kl, kl_r = kl_divergence(Pn, Y), kl_divergence(Pn, Yr)
+    assert abs(kl - kl_r) / kl_r < 0.01, (kl, kl_r)
+    assert abs(knn_overlap(g["X"], Y) - knn_overlap(g["X"], Yr)) < 0.02
+
+
 def test_device_loop_first_iteration_matches_kernels(mg, golden):
     """one iteration of the device loop equals the per-call sequence attraction -> FFT repulsion -> step"""
     g = golden("tsne_small.npz")
