@@ -113,3 +113,16 @@ def test_fft_sides_against_fp64(mg, M):
     sq64, F64 = O.fft_repulsion_fp64(Y, 0.0, 0.0, width, nb, n_interp=ni)
     assert abs(sq - sq64) / sq64 < TOL
     assert np.linalg.norm(F - F64) / np.linalg.norm(F64) < TOL
+
+
+@pytest.mark.parametrize("ni", [2, 4, 7])
+def test_other_interpolation_orders_against_fp64(mg, ni):
+    """FFTConv2D at interpolation orders other than 3 and 5 (the device instantiates 1-8) against the FP64
+    restatement of the pass, which matches the reference's FFTConv2D at these orders (tests/test_oracle.py)"""
+    rng = np.random.default_rng(ni)
+    Y = rng.normal(0, 8, (2500, 2)).astype(np.float32)
+    grid = O.grid(Y)
+    sq, F = fftconv(mg, Y, grid, ni)
+    sq_o, F_o = O.fft_repulsion_fp64(Y, *grid, ni)
+    assert abs(sq - sq_o) / abs(sq_o) < 1e-4
+    assert np.linalg.norm(F - F_o) / np.linalg.norm(F_o) < 1e-4

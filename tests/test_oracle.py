@@ -175,6 +175,24 @@ def test_fft_fp64_oracle_against_reference(golden, ni):
     assert np.linalg.norm(F - g["F_exact"]) / np.linalg.norm(g["F_exact"]) < 2e-2
 
 
+@pytest.mark.parametrize("ni", [2, 4, 7])
+def test_fft_fp64_oracle_other_orders(ref, ni):
+    """the FP64 restatement of the FFT pass against the reference's own FFTConv2D at interpolation orders
+    other than 3 and 5 (the reference run live; it computes in FP32)"""
+    if ref is None:
+        pytest.skip("reference module not built")
+    rng = np.random.default_rng(ni)
+    Y = rng.normal(0, 8, (2500, 2)).astype(np.float32)
+    xmin, ymin, width, nb = O.grid(Y)
+    M, K1, K2 = O.kernel_spectra(nb, width, ni)
+    conv = ref.FFTConv2D(M, ni)
+    conv.set_kernels(K1, K2)
+    sq_r, F_r = conv.compute(Y, xmin, ymin, width, nb, 1)
+    sq, F = O.fft_repulsion_fp64(Y, xmin, ymin, width, nb, ni)
+    assert abs(sq - sq_r) / abs(sq_r) < 1e-4
+    assert np.linalg.norm(F - np.asarray(F_r)) / np.linalg.norm(F) < 1e-4
+
+
 def test_exact_repulsion_oracle(golden):
     g = golden("fft_small.npz")
     sq, F = O.exact_repulsion(g["Y"])
