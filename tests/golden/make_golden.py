@@ -197,6 +197,8 @@ def graph_fixture():
         out["data" + suffix] = P.data.astype(np.float32)
     out["vals"] = np.asarray(_magnet.smooth_knn(dist, 15))
     out["vals_e"] = np.asarray(_magnet.smooth_knn(dist_e, 15))
+    from magnet.knn import rescale_neighbor_distances
+    out["dist_pow"] = rescale_neighbor_distances(dist, power=0.5, rank_exponent=0.25)
     np.savez_compressed(os.path.join(HERE, "graph_small.npz"), **out)
 
 

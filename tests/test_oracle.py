@@ -249,3 +249,11 @@ def test_served_request_stream_is_seeded():
     assert all(np.array_equal(x, z) for x, z in zip(s1[2], s2[2]))
     assert s1[0].min() >= 1 and s1[0].max() <= 4096 and (s1[1] > 0).all()
     assert sorted(len(v) for v in s1[3].values()) == [50, 80] and all(0 < k < 40 for k in s1[3])
+
+
+def test_neighbour_distance_rescale_matches_reference(golden):
+    """the package's host rescale of the distance profile (power, rank exponent) equals magnet/knn.py's
+    rescale_neighbor_distances bit for bit"""
+    from magnet_b200.graph import rescale_neighbor_distances
+    g = golden("graph_small.npz")
+    assert np.array_equal(rescale_neighbor_distances(g["dist"], power=0.5, rank_exponent=0.25), g["dist_pow"])
