@@ -6,7 +6,7 @@ by the reference's own code: its compiled `_magnet` (optimize_layout at n_thread
 tsne_attraction, tsne_step, bbox_2d, smooth_knn) and its Python drivers (magnet/tsne.py FFTRepulsion2D /
 optimize_tsne, magnet/knn.py fuzzy_graph, magnet/__init__.py edge schedule). Inputs are seeded synthetic data.
 
-    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner graph tsne_variants]
+    python tests/golden/make_golden.py [sgd fft tsne sgd_options sgd_owner graph tsne_variants params]
 """
 import os
 import sys
@@ -215,6 +215,15 @@ def tsne_variants_fixture():
     np.savez_compressed(os.path.join(HERE, "tsne_variants.npz"), **out)
 
 
+def params_fixture():
+    """the reference's find_ab_params (magnet/__init__.py:26-48) at the settings of sgd_cases.AB_CASES:
+    rows (a, b)"""
+    from magnet import find_ab_params
+    from sgd_cases import AB_CASES
+    np.savez_compressed(os.path.join(HERE, "params_small.npz"),
+                        ab=np.array([find_ab_params(**kw) for kw in AB_CASES], np.float64))
+
+
 def sgd_owner_fixture():
     """the reference's owner mode (parallel=1, 4 threads; its result does not depend on the thread count) on each
     owner case of sgd_cases.py: the final Y and sha-256 digests of eons, eonns and the Adam state at seed 12345,
@@ -241,10 +250,11 @@ def sgd_owner_fixture():
 
 if __name__ == "__main__":
     # all fixtures, or only those named on the command line (sgd_options reads sgd_small.npz)
-    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner", "graph", "tsne_variants"]
+    todo = sys.argv[1:] or ["sgd", "fft", "tsne", "sgd_options", "sgd_owner", "graph", "tsne_variants", "params"]
     for name in todo:
         {"sgd": sgd_fixture, "fft": fft_fixture, "tsne": tsne_fixture, "sgd_options": sgd_options_fixture,
-         "sgd_owner": sgd_owner_fixture, "graph": graph_fixture, "tsne_variants": tsne_variants_fixture}[name]()
+         "sgd_owner": sgd_owner_fixture, "graph": graph_fixture, "tsne_variants": tsne_variants_fixture,
+         "params": params_fixture}[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

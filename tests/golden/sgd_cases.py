@@ -181,3 +181,10 @@ def digest(a):
     """sha-256 of an array's bytes (C order), the compact form of bit-exact bookkeeping in the fixtures"""
     import hashlib
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+# settings of the kernel fit find_ab_params (magnet/__init__.py:26-48): the default, a given b (the bench's
+# size-dependent b), another spread, and the gaussian, sech and tanh kernels
+AB_CASES = [dict(spread=1.0, min_dist=0.1), dict(spread=1.0, min_dist=0.05, b=0.6),
+            dict(spread=1.5, min_dist=0.2), dict(spread=1.0, min_dist=0.1, kernel="gaussian"),
+            dict(spread=1.0, min_dist=0.1, kernel="sech"), dict(spread=1.0, min_dist=0.1, kernel="tanh")]

@@ -257,3 +257,25 @@ def test_neighbour_distance_rescale_matches_reference(golden):
     from magnet_b200.graph import rescale_neighbor_distances
     g = golden("graph_small.npz")
     assert np.array_equal(rescale_neighbor_distances(g["dist"], power=0.5, rank_exponent=0.25), g["dist_pow"])
+
+
+def test_edge_schedule_matches_reference(golden):
+    """the package's edge schedule (sampling frequencies, the drop rule, COO order) equals the reference's
+    MAGNET._edge_schedule (magnet/__init__.py:51-66, 727-737) on the same graph bit for bit"""
+    import scipy.sparse as sp
+    from magnet_b200 import drivers as D
+    g = golden("sgd_small.npz")
+    P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]))
+    head, tail, eps = D.edge_schedule(P, 40)
+    assert np.array_equal(head, g["head"]) and np.array_equal(tail, g["tail"]) and np.array_equal(eps, g["eps"])
+    h2, t2, e2 = O.edge_schedule(P, 40)
+    assert np.array_equal(h2, g["head"]) and np.array_equal(t2, g["tail"]) and np.array_equal(e2, g["eps"])
+
+
+def test_find_ab_params_matches_reference(golden):
+    """the package's kernel fit equals the reference's find_ab_params at six settings"""
+    from magnet_b200 import drivers as D
+    ab = golden("params_small.npz")["ab"]
+    for kw, (a, b) in zip(C.AB_CASES, ab):
+        got = D.find_ab_params(**kw)
+        assert np.allclose(got, (a, b), rtol=1e-10, atol=0), (kw, got, (a, b))
