@@ -200,7 +200,7 @@ class FittedLayout:
         candidates = 12 * mb * self.n_tiles * self.k
         return dist_block + candidates + 64 * m * self.k + 48 * (self.n + m)
 
-    def bind_stream(self, slot=None):
+    def bind_stream(self):
         """give this thread a CUDA stream of its own: torch's current stream for the thread, and the C ABI's"""
         st = self.torch.cuda.Stream(device=self.dev)
         self.torch.cuda.set_stream(st)
@@ -303,7 +303,7 @@ def device_server(layout, slots=4, budget_fraction=0.5):
 
     def init(slot):
         layout.torch.cuda.set_device(layout.dev)
-        layout.bind_stream(slot)
+        layout.bind_stream()
 
     def work(kind, payload, slot):
         if kind == "transform":
