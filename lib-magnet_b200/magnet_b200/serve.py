@@ -82,6 +82,7 @@ class Server:
         self.done = []
         self._done_lock = threading.Lock()
         self.peak_reserved = 0
+        self._healthy = self.slots   # slots whose start-up succeeded (or has not failed yet)
         self._threads = [threading.Thread(target=self._run, args=(s, init), daemon=True) for s in range(self.slots)]
         for t in self._threads:
             t.start()
@@ -113,8 +114,19 @@ class Server:
             self._cv.notify_all()
 
     def _run(self, slot, init):
+        init_error = None
         if init is not None:
-            init(slot)
+            try:
+                init(slot)
+            except BaseException as e:
+                init_error = e
+            with self._cv:
+                if init_error is not None:
+                    self._healthy -= 1
+                    # a slot that cannot start leaves the work to the others; the last one left fails the
+                    # requests instead of letting them wait forever
+                    if self._healthy > 0:
+                        return
         while True:
             r = self._q.get()
             if r is None:
@@ -122,6 +134,8 @@ class Server:
             self._admit(r)
             r.t_start = time.perf_counter()
             try:
+                if init_error is not None:
+                    raise RuntimeError("server slot %d failed to start: %s" % (slot, init_error))
                 res = self.work(r.kind, r.payload, slot)
                 r.t_done = time.perf_counter()
                 r.future.set_result(res)
@@ -238,6 +252,8 @@ class FittedLayout:
         """new rows (m, d) -> their layout positions (m, 2), on this thread's stream"""
         torch = self.torch
         from . import _native as N
+        if len(X_new) == 0:
+            return np.zeros((0, self.Yd.shape[1]), np.float32)
         st = getattr(_THREAD, "stream", None)
         if st is None:
             # a thread that is not a server worker: the caller's current stream, for torch and the C ABI alike

@@ -73,3 +73,26 @@ def test_failure_is_isolated_and_oversize_is_refused():
     with pytest.raises(ValueError, match="more than the server's budget"):
         srv.submit("t", (2, 0.0), nbytes=101)
     srv.close()
+
+
+def test_slot_that_fails_to_start_leaves_the_work_to_the_others():
+    """a worker whose start-up raises (e.g. its device cannot be set) takes no requests while another slot
+    works; when every slot fails, the requests fail instead of waiting forever"""
+    def init_one_bad(slot):
+        if slot == 0:
+            raise RuntimeError("no device for slot 0")
+
+    srv = Server(lambda kind, payload, slot: (payload, slot), slots=2, budget_bytes=100, init=init_one_bad)
+    futs = [srv.submit("t", i, nbytes=10) for i in range(20)]
+    assert [f.result(timeout=30) for f in futs] == [(i, 1) for i in range(20)]
+    srv.close()
+
+    def init_all_bad(slot):
+        raise RuntimeError("no device")
+
+    srv = Server(lambda kind, payload, slot: payload, slots=3, budget_bytes=100, init=init_all_bad)
+    futs = [srv.submit("t", i, nbytes=10) for i in range(5)]
+    for f in futs:
+        with pytest.raises(RuntimeError, match="failed to start"):
+            f.result(timeout=30)
+    srv.close()
