@@ -188,6 +188,16 @@ int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* sampled, int
  * log2(n_neighbors) * bandwidth in n_iter steps at most. */
 int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter, float* out);
 
+/* mid_near_pairs_dense (src/nndescent.cpp:731-768, bound at src/bindings.cpp:66-67): X (n, d) dense rows -> out
+ * (n, n_pairs), for every row and pair the second closest, by squared distance then index, of n_cand rows drawn
+ * at random (the row itself replaced by the next row). The draws are the reference's streams for n_threads threads
+ * (<= 0: the host's hardware threads, as the reference resolves it; the partners depend on it as the reference's
+ * do) and the squared distances follow the reference's kernel for the host's instruction set, so out equals the
+ * reference's output for the same n_threads on the same host. n_pairs >= 1, n_cand >= 2 and n > n_cand
+ * (MG_ERR_ARGUMENT otherwise, with the reference's message). Synchronous. */
+int mg_mid_near_pairs(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed, int n_threads,
+                      int32_t* out);
+
 /* The fuzzy union of fuzzy_graph (magnet/knn.py:215-230, after smooth_knn): A = the n x n matrix with rows
  * i < n_rows holding (ind[i, j], vals[i, j]) (duplicate columns summed, zeros dropped), and
  * P = mix (A + A^T - A o A^T) + (1 - mix) (A o A^T) with mix = set_op_mix_ratio, zeros dropped, columns sorted.

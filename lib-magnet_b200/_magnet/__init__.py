@@ -2,19 +2,19 @@
 
 Put the directory holding this package ahead of the reference's extension on sys.path; the reference's Python
 package (`magnet`) then runs its layout pass on the B200: optimize_layout, FFTConv2D, tsne_attraction, tsne_step,
-tsne_update, bbox_2d, mid_spring and smooth_knn come from the device library. The host-side kernels that stay on
-the reference's code (nn_descent, knn_search, mid-near pairs, spectral init, louvain) are forwarded to
-the reference's own compiled module, found through the MAGNET_HOST_MODULE environment variable (path to the
-reference's `_magnet*.so`); without it they raise ImportError when used, as a missing `_magnet` would.
+tsne_update, bbox_2d, mid_spring, smooth_knn and mid_near_pairs_dense come from the device library. The host-side
+kernels that stay on the reference's code (nn_descent, knn_search, sparse mid-near pairs, spectral init, louvain)
+are forwarded to the reference's own compiled module, found through the MAGNET_HOST_MODULE environment variable
+(path to the reference's `_magnet*.so`); without it they raise ImportError when used, as a missing `_magnet` would.
 """
 import importlib.util as _ilu
 import os as _os
+import sys as _sys
 
 from magnet_b200._native import (FFTConv2D, optimize_layout, tsne_attraction, tsne_step, tsne_update,  # noqa: F401
-                                 bbox_2d, mid_spring, smooth_knn)
+                                 bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense)
 
-_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search", "knn_search_sparse", "mid_near_pairs_dense",
-               "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration", "louvain", "interp_scatter",
+_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search", "knn_search_sparse", "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration", "louvain", "interp_scatter",
                "interp_gather", "scatter_padded_2d", "spectral_products", "gather_forces_2d", "umap_attraction")
 
 
@@ -22,6 +22,12 @@ def _load_host():
     path = _os.environ.get("MAGNET_HOST_MODULE")
     if not path:
         return None
+    # a module already loaded from the same file is reused: initialising a pybind11 extension twice in one
+    # process registers its types twice
+    for m in list(_sys.modules.values()):
+        f = getattr(m, "__file__", None)
+        if f and _os.path.realpath(f) == _os.path.realpath(path):
+            return m
     spec = _ilu.spec_from_file_location("magnet_host_native._magnet", path)
     mod = _ilu.module_from_spec(spec)
     spec.loader.exec_module(mod)

@@ -672,6 +672,26 @@ extern "C" int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbor
     });
 }
 
+extern "C" int mg_mid_near_pairs(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed,
+                                 int n_threads, int32_t* out) {
+    return guard([&] {
+        require(X && out && d >= 1, "X must be 2-d");
+        // src/nndescent.cpp:737
+        require(n_pairs >= 1 && n_cand >= 2 && n >= n_cand + 1, "need n_pairs >= 1, n_cand >= 2 and n > n_cand");
+        require(n <= INT32_MAX, "n must fit 32-bit indices");
+        if (n_threads <= 0) {   // the reference's resolve(): all hardware threads, 4 when unknown
+            const unsigned h = std::thread::hardware_concurrency();
+            n_threads = h == 0 ? 4 : (int)h;
+        }
+        cudaStream_t s = current_stream();
+        const float* Xd = in_dev(X, n * (int64_t)d, 0, s);
+        int32_t* od = out_dev(out, n * (int64_t)n_pairs, 1);
+        mid_near_pairs_dev(Xd, n, d, n_pairs, n_cand, seed, n_threads, host_distance_order(), od, graph_work(), s);
+        back(out, od, n * (int64_t)n_pairs, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 extern "C" int mg_fuzzy_union(const int32_t* ind, const float* vals, int64_t n_rows, int k, int64_t n,
                               double set_op_mix_ratio, int32_t* indptr, int32_t* indices, float* data, int64_t cap,
                               int64_t* nnz) {

@@ -8,6 +8,7 @@ namespace mgb {
 // device scratch of the graph passes
 struct GraphWork {
     DevBuf sigma, rho, part, acol, aval, alen, tcnt, tptr, tcur, trow, tval, ucnt, uptr, scan, flag;
+    DevBuf mid_state, mid_tab;   // mid-near partners: per-row stream states, jump tables and chunk tables
 };
 
 // memberships (n_rows, k) of sorted neighbour distances; `target` = log2(n_neighbors) * bandwidth, computed by the
@@ -20,5 +21,13 @@ void smooth_knn_dev(const float* dist, int64_t n_rows, int k, float target, int 
 int64_t fuzzy_union_dev(const int32_t* ind, const float* vals, int64_t n_rows, int k, int64_t n, float mix,
                         float one_minus_mix, int32_t* indptr, int32_t* indices, float* data, int64_t cap,
                         GraphWork& w, cudaStream_t s);
+
+// Mid-near partners of dense rows X (n, d) (src/nndescent.cpp:731-768): out (n, n_pairs), for every row and pair
+// the second closest (squared distance, index) of n_cand draws, with the reference's streams for `n_threads`
+// threads (>= 1) and its squared-distance kernel `order` (0 AVX-512, 1 AVX2, 2 plain loop).
+void mid_near_pairs_dev(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed, int n_threads,
+                        int order, int32_t* out, GraphWork& w, cudaStream_t s);
+// the reference's distance kernel on this host (its CPUID choice, src/nndescent.cpp:101-106)
+int host_distance_order();
 
 }  // namespace mgb

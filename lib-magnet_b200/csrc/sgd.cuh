@@ -33,7 +33,8 @@ struct SgdDev {
 // device scratch of the stream modes and of owner mode
 struct SgdWork {
     DevBuf cnt, state, delta, eptr, flag;
-    DevBuf samp;               // the epoch's per-edge negatives counts (counter mode fast path)
+    DevBuf samp;               // the epoch's sampled set (counter mode fast path)
+    DevBuf ctr;                // row counter of the flat sample kernel
     // owner mode: node rows, chunk bounds, per-edge negatives, per-node stream states, marked chunks, snapshots
     DevBuf o_row, o_own, o_neg, o_state, o_dirty, o_snap, o_snap_m, o_snap_v, o_snap_t;
 };

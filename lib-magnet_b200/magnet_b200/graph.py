@@ -1,13 +1,15 @@
 """Host-side inputs of the layout pass: the fuzzy neighbour graph, mid-near partners and the initial layout.
 
-These steps are upstream of the layout pass. The fuzzy graph runs on the device; the others are restated here
-on the host, from the reference's behaviour, so that workloads can be built where the reference is not installed:
+These steps are upstream of the layout pass. The fuzzy graph and the mid-near partners run on the device; the
+others are restated here on the host, from the reference's behaviour, so that workloads can be built where the
+reference is not installed:
 
 * ``smooth_knn``: UMAP's per-row bandwidth search (src/graph.cpp:29-78), on the device;
 * ``fuzzy_graph``: the fuzzy union A + A^T - A o A^T (magnet/knn.py:215-230), on the device;
 * ``exact_knn``: exact k nearest neighbours (self excluded, sorted) by blocked matmul on a CUDA device when
   torch sees one, else numpy; it stands in for NN-descent (src/nndescent.cpp), whose output it bounds;
-* ``mid_near_pairs``: PaCMAP-style partners, the second closest of n_cand random rows (src/nndescent.cpp:731-759);
+* ``mid_near_pairs``: PaCMAP-style partners, the second closest of n_cand random rows (src/nndescent.cpp:731-759),
+  on the device with the reference's streams and distance arithmetic;
 * ``initial_layout``: the reference's rescale of an initial embedding (magnet/__init__.py:444-448).
 """
 import numpy as np
@@ -90,21 +92,14 @@ def exact_knn(X, k, block=2048):
     return I, D
 
 
-def mid_near_pairs(X, n_pairs=5, n_cand=6, seed=0, block=65536):
-    """(n, n_pairs) int32: for every row and pair, the second closest of n_cand random other rows"""
-    X = np.ascontiguousarray(X, dtype=np.float32)
-    n = X.shape[0]
-    rng = np.random.default_rng(seed)
-    out = np.empty((n, n_pairs), np.int32)
-    for s in range(0, n, block):
-        e = min(n, s + block)
-        rows = np.arange(s, e)
-        cand = rng.integers(0, n - 1, (e - s, n_pairs, n_cand))
-        cand = cand + (cand >= rows[:, None, None])          # never the row itself
-        d = ((X[cand] - X[rows][:, None, None, :]) ** 2).sum(-1)
-        second = np.argsort(d, axis=-1)[..., 1]
-        out[s:e] = np.take_along_axis(cand, second[..., None], -1)[..., 0]
-    return out
+def mid_near_pairs(X, n_pairs=5, n_cand=6, seed=0, n_threads=-1):
+    """(n, n_pairs) int32 PaCMAP-style partners on the device (magnet/roles.py:36-51 over src/nndescent.cpp:731-768):
+    for every row and pair, the second closest of n_cand rows drawn with the reference's streams for n_threads
+    threads (-1: the host's hardware threads, as the reference resolves it), so the partners are the reference's
+    own for the same thread count"""
+    from . import _native
+    return _native.mid_near_pairs_dense(np.ascontiguousarray(X, dtype=np.float32), int(n_pairs), int(n_cand),
+                                        int(seed), int(n_threads))
 
 
 def pca2(X, seed=0):

@@ -246,6 +246,19 @@ py::array_t<float> smooth_knn(py::object dist, int n_neighbors, float bandwidth,
     return out;
 }
 
+// mid_near_pairs_dense of src/nndescent.cpp:731-768 on the device (signature of src/bindings.cpp:66-67)
+py::array_t<int32_t> mid_near_pairs_dense(py::object X, int n_pairs, int n_cand, uint64_t seed, int n_threads) {
+    auto x = view<float>(X);
+    if (x.ndim() != 2 || x.dim(1) < 1) throw std::runtime_error("X must be 2-d");
+    const int64_t n = x.dim(0);
+    py::array_t<int32_t> out({n, (int64_t)n_pairs});
+    {
+        py::gil_scoped_release rel;
+        check(mg_mid_near_pairs(x.ptr, n, (int)x.dim(1), n_pairs, n_cand, seed, n_threads, out.mutable_data()));
+    }
+    return out;
+}
+
 // the fuzzy union of magnet/knn.py:221-230 on the device: (indptr, indices, data) of the n x n CSR
 py::tuple fuzzy_union(py::object ind, py::object vals, int64_t n, double set_op_mix_ratio) {
     auto id = view<int32_t>(ind);
@@ -302,6 +315,8 @@ PYBIND11_MODULE(_native, m) {
     m.def("smooth_knn", &smooth_knn, "UMAP smooth-kNN memberships (n, k) from sorted neighbour distances (device)",
           py::arg("dist"), py::arg("n_neighbors"), py::arg("bandwidth") = 1.0f, py::arg("n_iter") = 64,
           py::arg("n_threads") = -1);
+    m.def("mid_near_pairs_dense", &mid_near_pairs_dense, "PaCMAP-style mid-near partners (dense rows, device)",
+          py::arg("X"), py::arg("n_pairs") = 5, py::arg("n_cand") = 6, py::arg("seed") = 0, py::arg("n_threads") = -1);
     m.def("fuzzy_union", &fuzzy_union, "fuzzy union A + A^T - A o A^T of kNN memberships (device): (indptr, indices, data)",
           py::arg("ind"), py::arg("vals"), py::arg("n") = -1, py::arg("set_op_mix_ratio") = 1.0);
     m.def("tsne_attraction", [](py::object indptr, py::object indices, py::object data, py::object Y, float dof, int) {

@@ -22,6 +22,7 @@
  *   orc_tsne_attraction src/fftrep.cpp:129-177
  *   orc_tsne_step       src/fftrep.cpp:225-266 (one thread: nt = 1 partial sums, i.e. blocks of 1024 rows)
  *   orc_bbox_2d         src/fftrep.cpp:415-434
+ *   orc_mid_near_pairs  src/nndescent.cpp:731-759 (mid_near_core, dense rows) with the distance kernels of :35-106
  *   orc_exact_repulsion FP64 all-pairs sumQ and F (the brute force of tests/test_magnet.py:221-231 and
  *                       benchmarks/theory/k16_fft_check.py:9-16), the precision oracle of the FFT pass
  */
@@ -781,4 +782,74 @@ void orc_bbox_2d(const float* Y, int64_t n, float* out4) {
         y0 = fminf(y0, Y[2 * i + 1]); y1 = fmaxf(y1, Y[2 * i + 1]);
     }
     out4[0] = x0; out4[1] = y0; out4[2] = x1; out4[3] = y1;
+}
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Mid-near partners, src/nndescent.cpp:731-759 (mid_near_core over dense rows): nt = min(n_threads, max(1, n / 2048))
+ * streams, stream t = Rng(seed + 48271 (t + 1)) over rows [n t / nt, n (t + 1) / nt); per row and pair, n_cand draws
+ * j = below(n) (j == i -> (j + 1) % n) with their squared distances, the second smallest (distance, index) is kept.
+ * The squared distance follows the reference's kernel for the host's instruction set (src/nndescent.cpp:35-116,
+ * chosen at :101-106): order 0 the AVX-512 kernel (16 lanes of fused multiply-adds, the lanes summed high half
+ * onto low half down to one, then the tail with fused multiply-adds), order 1 the AVX2 kernel (8 lanes, the lanes
+ * summed ((0+1)+(2+3))+((4+5)+(6+7)), then the tail), order 2 the plain loop (4 interleaved sums, no fusion).
+ * Order 0 equals the reference's distances bit for bit (checked against its nn_descent output). */
+static float orc_sqdist(const float* a, const float* b, int d, int order) {
+    if (order == 2) {
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+        int i = 0;
+        for (; i + 4 <= d; i += 4) {
+            const float d0 = a[i] - b[i], d1 = a[i + 1] - b[i + 1], d2 = a[i + 2] - b[i + 2], d3 = a[i + 3] - b[i + 3];
+            s0 += d0 * d0; s1 += d1 * d1; s2 += d2 * d2; s3 += d3 * d3;
+        }
+        for (; i < d; ++i) { const float df = a[i] - b[i]; s0 += df * df; }
+        return (s0 + s1) + (s2 + s3);
+    }
+    const int L = order == 0 ? 16 : 8;
+    float acc[16] = {0};
+    int i = 0;
+    for (; i + L <= d; i += L)
+        for (int l = 0; l < L; ++l) { const float df = a[i + l] - b[i + l]; acc[l] = fmaf(df, df, acc[l]); }
+    float s;
+    if (order == 0) {
+        float t3[8], t6[4];
+        for (int k = 0; k < 8; ++k) t3[k] = acc[8 + k] + acc[k];
+        for (int k = 0; k < 4; ++k) t6[k] = t3[4 + k] + t3[k];
+        s = (t6[0] + t6[2]) + (t6[1] + t6[3]);
+    } else {
+        s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    }
+    for (; i < d; ++i) { const float df = a[i] - b[i]; s = fmaf(df, df, s); }
+    return s;
+}
+
+int orc_mid_near_pairs(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed, int n_threads,
+                       int order, int32_t* out) {
+    if (!(n_pairs >= 1 && n_cand >= 2 && n >= n_cand + 1)) return 1;
+    int64_t nt = n / 2048 > 1 ? n / 2048 : 1;
+    if (n_threads < nt) nt = n_threads;
+    float* dist = (float*)malloc(sizeof(float) * n_cand);
+    int32_t* idx = (int32_t*)malloc(sizeof(int32_t) * n_cand);
+    for (int64_t t = 0; t < nt; ++t) {
+        orc_rng rng;
+        orc_rng_seed(&rng, seed + 48271ULL * (uint64_t)(t + 1));
+        const int64_t r0 = n * t / nt, r1 = n * (t + 1) / nt;
+        for (int64_t i = r0; i < r1; ++i)
+            for (int p = 0; p < n_pairs; ++p) {
+                for (int c = 0; c < n_cand; ++c) {
+                    int32_t j = (int32_t)orc_rng_below(&rng, (uint32_t)n);
+                    if (j == i) j = (int32_t)((j + 1) % n);
+                    idx[c] = j;
+                    dist[c] = orc_sqdist(X + i * d, X + (int64_t)j * d, d, order);
+                }
+                /* the two smallest (distance, index) pairs in order; the second is kept */
+                int b0 = -1, b1 = -1;
+                for (int c = 0; c < n_cand; ++c) {
+                    if (b0 < 0 || dist[c] < dist[b0] || (dist[c] == dist[b0] && idx[c] < idx[b0])) { b1 = b0; b0 = c; }
+                    else if (b1 < 0 || dist[c] < dist[b1] || (dist[c] == dist[b1] && idx[c] < idx[b1])) b1 = c;
+                }
+                out[i * n_pairs + p] = idx[b1];
+            }
+    }
+    free(dist); free(idx);
+    return 0;
 }

@@ -97,6 +97,9 @@ def lib():
         L.orc_tsne_attraction.argtypes = [_P, _P, _P, _P, _I64, ctypes.c_int, _F, _P]
         L.orc_tsne_step.argtypes = [_P, _P, _P, _P, _P, _I64, ctypes.c_int, _F, _F, _F, _F]
         L.orc_bbox_2d.argtypes = [_P, _I64, _P]
+        L.orc_mid_near_pairs.argtypes = [_P, _I64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                         ctypes.c_int, ctypes.c_int, _P]
+        L.orc_mid_near_pairs.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -394,6 +397,30 @@ def optimize_sgd(Y, head, tail, eps, n_epochs, *, lr=1.0, mid_weight=0.0, mid_ph
     return Y
 
 
+def host_distance_order():
+    """the reference's squared-distance kernel on this host (src/nndescent.cpp:101-106): 0 AVX-512, 1 AVX2 + FMA,
+    2 the plain loop"""
+    try:
+        flags = set(open("/proc/cpuinfo").read().split())
+    except OSError:
+        return 2
+    return 0 if "avx512f" in flags else (1 if {"avx2", "fma"} <= flags else 2)
+
+
+def mid_near_pairs(X, n_pairs=5, n_cand=6, seed=0, n_threads=-1, order=None):
+    """mid_near_pairs_dense (src/nndescent.cpp:731-768) restated in C: (n, n_pairs) int32. n_threads -1 means the
+    host's hardware threads, as the reference resolves it; order: the distance kernel (host_distance_order())"""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n, d = X.shape
+    nt = n_threads if n_threads > 0 else (os.cpu_count() or 4)
+    out = np.empty((n, n_pairs), np.int32)
+    rc = lib().orc_mid_near_pairs(_ptr(X), n, d, int(n_pairs), int(n_cand), int(seed), int(nt),
+                                  host_distance_order() if order is None else int(order), _ptr(out))
+    if rc != 0:
+        raise RuntimeError("need n_pairs >= 1, n_cand >= 2 and n > n_cand")
+    return out
+
+
 def find_ab_params(spread=1.0, min_dist=0.1):
     """magnet/__init__.py:26-48, the power kernel: a, b of 1 / (1 + a d^(2b)) fitted to the (min_dist, spread)
     curve"""
@@ -496,59 +523,86 @@ def reference_transform(X_train, P, Y_train, landmarks, step, Q, *, a, b, n_neig
     return Y_all[n_train:]
 
 
+class TsneRun:
+    """The loop of magnet/tsne.py:132-184 (the common path: no mid-range or far-field terms) as a resumable run:
+    the set-up of the reference's driver (P normalised to sum 1, the learning rate, zero update, unit gains, the
+    spectrum and FFTConv2D caches) once, then ``advance(k)`` runs the next k iterations with the same state, so a
+    long pass can be timed in pieces. backend "reference" drives the compiled reference's kernels, "oracle" the C
+    restatement with the FP64 convolution."""
+
+    def __init__(self, P, Y, n_iter=750, early_iter=250, early_exaggeration=12.0, exaggeration=1.0,
+                 learning_rate=None, momentum=(0.5, 0.8), n_interp=3, box_width=0.7, n_threads=-1, dof=1.0,
+                 backend="reference", callback=None):
+        import scipy.sparse as sp
+        n = P.shape[0]
+        P = sp.csr_matrix(P, dtype=np.float32)
+        P = P / P.sum()
+        self.indptr, self.indices, self.data = (P.indptr.astype(np.int32), P.indices.astype(np.int32),
+                                                P.data.astype(np.float32))
+        self.lr = max(200.0, n / early_exaggeration) if learning_rate is None else learning_rate
+        self.Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self.update = np.zeros_like(self.Y)
+        self.gains = np.ones_like(self.Y)
+        self.R = reference() if backend == "reference" else None
+        self.convs, self.spectra = {}, {}
+        self.it = 0
+        self.n_iter, self.early_iter = n_iter, early_iter
+        self.early_exaggeration, self.exaggeration, self.momentum = early_exaggeration, exaggeration, momentum
+        self.n_interp, self.box_width, self.n_threads, self.dof = n_interp, box_width, n_threads, dof
+        self.callback = callback
+
+    def advance(self, k):
+        """runs iterations it .. min(it + k, n_iter) - 1; returns Y (updated in place)"""
+        R, Y, update, gains = self.R, self.Y, self.update, self.gains
+        indptr, indices, data = self.indptr, self.indices, self.data
+        n_interp, box_width, n_threads, dof = self.n_interp, self.box_width, self.n_threads, self.dof
+        for it in range(self.it, min(self.it + k, self.n_iter)):
+            early = it < self.early_iter
+            rho = self.early_exaggeration if early else self.exaggeration
+            mom = self.momentum[0] if early else self.momentum[1]
+            if R is not None:
+                attr = np.asarray(R.tsne_attraction(indptr, indices, data, Y, float(dof), n_threads))
+                xmin, ymin, xmax, ymax = R.bbox_2d(Y, n_threads)
+                lo = np.array([xmin, ymin]) - 1e-3
+                hi = np.array([xmax, ymax]) + 1e-3
+                span = float((hi - lo).max())
+                n_boxes = int(np.clip(np.ceil(span / box_width), 20, 1000))
+                n_boxes = min(1000, -(-n_boxes // 4) * 4)
+                width = box_width if n_boxes * box_width >= span else max(span / n_boxes, 1e-12)
+                key = (n_boxes, round(width, 6))
+                if key not in self.spectra:
+                    if len(self.spectra) > 8:
+                        self.spectra.pop(next(iter(self.spectra)))
+                    self.spectra[key] = kernel_spectra(n_boxes, width, n_interp, dof)
+                M, K1, K2 = self.spectra[key]
+                ck = (M, round(width, 6))
+                conv = self.convs.get(ck)
+                if conv is None:
+                    conv = R.FFTConv2D(int(M), n_interp)
+                    conv.set_kernels(K1, K2)
+                    if len(self.convs) > 4:
+                        self.convs.pop(next(iter(self.convs)))
+                    self.convs[ck] = conv
+                sumQ, F = conv.compute(Y, float(lo[0]), float(lo[1]), width, n_boxes, n_threads)
+                R.tsne_step(Y, update, gains, attr, np.asarray(F), float(rho), float(1.0 / max(sumQ, 1e-12)),
+                            float(self.lr), float(mom), n_threads)
+            else:
+                attr = tsne_attraction(indptr, indices, data, Y, dof)
+                xmin, ymin, width, n_boxes = grid(Y, box_width)
+                sumQ, F = fft_repulsion_fp64(Y, xmin, ymin, width, n_boxes, n_interp, dof)
+                tsne_step(Y, update, gains, attr, F.astype(np.float32), float(rho), float(1.0 / max(sumQ, 1e-12)),
+                          float(self.lr), float(mom))
+            if self.callback is not None:
+                self.callback(it, Y)
+        self.it = min(self.it + k, self.n_iter)
+        return Y
+
+
 def optimize_tsne(P, Y, n_iter=750, early_iter=250, early_exaggeration=12.0, exaggeration=1.0,
                   learning_rate=None, momentum=(0.5, 0.8), n_interp=3, box_width=0.7, n_threads=-1,
                   dof=1.0, backend="reference", callback=None):
     """magnet/tsne.py:132-184 (the common path: no mid-range or far-field terms), driving the compiled
     reference's kernels (backend "reference") or the C restatement with the FP64 convolution ("oracle")."""
-    import scipy.sparse as sp
-    n = P.shape[0]
-    P = sp.csr_matrix(P, dtype=np.float32)
-    P = P / P.sum()
-    indptr, indices, data = P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data.astype(np.float32)
-    if learning_rate is None:
-        learning_rate = max(200.0, n / early_exaggeration)
-    Y = np.ascontiguousarray(Y, dtype=np.float32)
-    update = np.zeros_like(Y)
-    gains = np.ones_like(Y)
-    R = reference() if backend == "reference" else None
-    convs, spectra = {}, {}
-    for it in range(n_iter):
-        early = it < early_iter
-        rho = early_exaggeration if early else exaggeration
-        mom = momentum[0] if early else momentum[1]
-        if R is not None:
-            attr = np.asarray(R.tsne_attraction(indptr, indices, data, Y, float(dof), n_threads))
-            xmin, ymin, xmax, ymax = R.bbox_2d(Y, n_threads)
-            lo = np.array([xmin, ymin]) - 1e-3
-            hi = np.array([xmax, ymax]) + 1e-3
-            span = float((hi - lo).max())
-            n_boxes = int(np.clip(np.ceil(span / box_width), 20, 1000))
-            n_boxes = min(1000, -(-n_boxes // 4) * 4)
-            width = box_width if n_boxes * box_width >= span else max(span / n_boxes, 1e-12)
-            key = (n_boxes, round(width, 6))
-            if key not in spectra:
-                if len(spectra) > 8:
-                    spectra.pop(next(iter(spectra)))
-                spectra[key] = kernel_spectra(n_boxes, width, n_interp, dof)
-            M, K1, K2 = spectra[key]
-            ck = (M, round(width, 6))
-            conv = convs.get(ck)
-            if conv is None:
-                conv = R.FFTConv2D(int(M), n_interp)
-                conv.set_kernels(K1, K2)
-                if len(convs) > 4:
-                    convs.pop(next(iter(convs)))
-                convs[ck] = conv
-            sumQ, F = conv.compute(Y, float(lo[0]), float(lo[1]), width, n_boxes, n_threads)
-            R.tsne_step(Y, update, gains, attr, np.asarray(F), float(rho), float(1.0 / max(sumQ, 1e-12)),
-                        float(learning_rate), float(mom), n_threads)
-        else:
-            attr = tsne_attraction(indptr, indices, data, Y, dof)
-            xmin, ymin, width, n_boxes = grid(Y, box_width)
-            sumQ, F = fft_repulsion_fp64(Y, xmin, ymin, width, n_boxes, n_interp, dof)
-            tsne_step(Y, update, gains, attr, F.astype(np.float32), float(rho), float(1.0 / max(sumQ, 1e-12)),
-                      float(learning_rate), float(mom))
-        if callback is not None:
-            callback(it, Y)
-    return Y
+    run = TsneRun(P, Y, n_iter, early_iter, early_exaggeration, exaggeration, learning_rate, momentum, n_interp,
+                  box_width, n_threads, dof, backend, callback)
+    return run.advance(n_iter)

@@ -279,3 +279,14 @@ def test_find_ab_params_matches_reference(golden):
     for kw, (a, b) in zip(C.AB_CASES, ab):
         got = D.find_ab_params(**kw)
         assert np.allclose(got, (a, b), rtol=1e-10, atol=0), (kw, got, (a, b))
+
+
+@pytest.mark.parametrize("n,d,nt,seed", [(5000, 50, 1, 0), (9000, 50, 3, 11), (6000, 10, 2, 5), (3000, 17, 1, 3)])
+def test_mid_near_pairs_oracle_matches_reference(ref, n, d, nt, seed):
+    """the C restatement of mid_near_core (src/nndescent.cpp:731-759), the host's distance kernel, against the
+    reference's compiled mid_near_pairs_dense: the same partners bit for bit"""
+    if ref is None:
+        pytest.skip("reference module not built")
+    rng = np.random.default_rng(n + d)
+    X = rng.normal(0, 3, (n, d)).astype(np.float32)
+    assert np.array_equal(np.asarray(ref.mid_near_pairs_dense(X, 5, 6, seed, nt)), O.mid_near_pairs(X, 5, 6, seed, nt))
