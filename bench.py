@@ -10,11 +10,14 @@ weight 0.2), recentre + rescale to std 31 sqrt(n / 70000), 300 full-batch FFT-re
 
 value: seconds per layout with every input already resident in HBM (lower is better). e2e: the same pass through
 the reference-shaped numpy API (optimize_layout / optimize_tsne with host arrays in pinned memory), host-device
-copies included. cpu_baseline / --impl reference: the reference's own CPU implementation (its compiled module,
-all host threads) timed on a bounded sample of the same workload (2 SGD epochs at mid-run sampling density and
-2 full-batch iterations at the hybrid pass's grid) and extrapolated to the whole pass.
+copies included. cpu_baseline: the reference's own CPU implementation (its compiled module, all host threads) on a
+bounded sample of the same workload (SGD epochs at mid-run sampling density and full-batch iterations at the pass's
+grid), extrapolated to the whole pass. --impl reference: the reference's CPU path alone, on inputs its own code
+builds (NN-descent, smooth_knn and the scipy union, its mid-near partners), timing one whole pass cut into the
+--steps pieces; nothing of this repository's native code is loaded in that process.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n N]
+    python bench.py --config 1|2|4 [--impl reference] [--steps K] [--warmup W]   (the other configurations)
     python bench.py --graph [--n N] [--steps K] [--warmup W] [--no-cpu-baseline]   (the fuzzy neighbour graph)
 
 transform / transform_plain: the served form (magnet_b200.serve) on a resident 200k x 64 layout: p50 / p99
@@ -62,7 +65,50 @@ def make_data(n, d=50, k=100, seed=2):
     return X[perm], labels[perm]
 
 
+def find_ab(spread, min_dist, b=None):
+    """the power kernel's (a, b) fitted to the (min_dist, spread) curve, b fixed when given (magnet/__init__.py:26-48);
+    both arms take the pass's parameters from here"""
+    from scipy.optimize import curve_fit
+    xv = np.linspace(0, spread * 3, 300)
+    yv = np.zeros(xv.shape)
+    yv[xv < min_dist] = 1.0
+    yv[xv >= min_dist] = np.exp(-(xv[xv >= min_dist] - min_dist) / spread)
+    if b is None:
+        params, _ = curve_fit(lambda x, a, bb: 1.0 / (1.0 + a * x ** (2 * bb)), xv, yv)
+        return float(params[0]), float(params[1])
+    params, _ = curve_fit(lambda x, a: 1.0 / (1.0 + a * x ** (2 * b)), xv, yv, p0=[1.0])
+    return float(params[0]), float(b)
+
+
+def pca_init(X, seed=2):
+    """the initial layout of both arms: a 2-D PCA projection (randomised range finder) rescaled as the reference
+    rescales its initial embedding (centred, max-abs 10, N(0, 1e-4) jitter; magnet/__init__.py:444-448). It stands
+    in for the spectral init, which stays on the reference's host code."""
+    Xc = X - X.mean(0)
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(Xc @ rng.normal(size=(X.shape[1], 8)).astype(np.float32))
+    for _ in range(2):
+        Q, _ = np.linalg.qr(Xc @ (Xc.T @ Q))
+    _, _, Vt = np.linalg.svd(Q.T @ Xc, full_matrices=False)
+    Y = (Xc @ Vt[:2].T).astype(np.float32)
+    Y -= Y.mean(0)
+    Y *= np.float32(10.0 / max(float(np.abs(Y).max()), 1e-30))
+    Y += np.random.default_rng(seed).normal(0, 1e-4, Y.shape).astype(np.float32)
+    return np.ascontiguousarray(Y, dtype=np.float32)
+
+
+def pass_params(n, seed=2):
+    """the loss="hybrid" defaults at n points: kernel_b "size" (magnet/__init__.py:561-565), min_dist 0.05, the
+    coupled repulsion exponent 1, the SGD seed drawn from random_state (:548-549)"""
+    kb = float(np.clip(0.6 + 0.2 * (np.log(20000.0) - np.log(max(n, 1))) / np.log(2.0), 0.6, 0.8))
+    a, b = find_ab(1.0, 0.05, kb)
+    rep_a, rep_b = find_ab(1.0, 0.05, 1.0)
+    return dict(a=a, b=b, rep_a=rep_a, rep_b=rep_b, seed=int(np.random.default_rng(seed).integers(0, 2 ** 62)))
+
+
 def make_workload(n, seed=2):
+    """the GPU arm's inputs: exact kNN, the fuzzy graph and the mid-near partners on the device (the partners are the
+    reference's own for the host's thread count), the reference's edge schedule"""
     import magnet_b200 as mg
     from magnet_b200 import graph as G
     t0 = time.time()
@@ -70,19 +116,362 @@ def make_workload(n, seed=2):
     ind, dist = G.exact_knn(X, 15)
     P = G.fuzzy_graph(ind, dist, 15)
     head, tail, eps = mg.edge_schedule(P, N_EPOCHS)
-    pairs = G.mid_near_pairs(X, 5, 6, seed=seed, block=16384)
-    Y0 = G.initial_layout(G.pca2(X, seed), seed)
-    kb = float(np.clip(0.6 + 0.2 * (np.log(20000.0) - np.log(max(n, 1))) / np.log(2.0), 0.6, 0.8))
-    a, b = mg.find_ab_params(1.0, 0.05, kb)
-    rep_a, rep_b = mg.find_ab_params(1.0, 0.05, 1.0)
-    sgd_seed = int(np.random.default_rng(seed).integers(0, 2 ** 62))
-    return dict(X=X, labels=labels, P=P, head=head, tail=tail, eps=eps, pairs=pairs, Y0=Y0, a=a, b=b, rep_a=rep_a,
-                rep_b=rep_b, seed=sgd_seed, n=n, setup_s=time.time() - t0)
+    pairs = G.mid_near_pairs(X, 5, 6, seed=seed, n_threads=-1)
+    Y0 = pca_init(X, seed)
+    return dict(X=X, labels=labels, P=P, head=head, tail=tail, eps=eps, pairs=pairs, Y0=Y0, n=n,
+                setup_s=time.time() - t0, graph="exact kNN (device)") | pass_params(n, seed)
+
+
+def make_workload_reference(n, seed=2, n_threads=-1):
+    """the reference arm's inputs, from the reference's own CPU code only: its NN-descent kNN with the parameters of
+    magnet/knn.py:90-122, its smooth_knn and the scipy union of magnet/knn.py:215-230, the edge schedule of
+    magnet/__init__.py:727-737 and its mid-near partners (src/nndescent.cpp:731-759)"""
+    from oracle import oracle as O
+    R = O.reference()
+    if R is None:
+        raise RuntimeError("the reference module (oracle/_ref) is not built")
+    t0 = time.time()
+    X, labels = make_data(n, seed=seed)
+    kin = min(max(14, 20), n - 1)
+    n_trees = int(max(2, min(8, round(np.sqrt(n) / 40))))
+    ind, d2 = R.nn_descent(X, int(kin), 50, 10, 0.001, n_trees, 30, int(seed), int(n_threads), False)
+    ind = np.asarray(ind)[:, :14].astype(np.int64)
+    dist = np.sqrt(np.maximum(np.asarray(d2)[:, :14], 0.0)).astype(np.float32)
+    P = O.reference_fuzzy_graph(ind, dist, 15, n_threads)
+    head, tail, eps = O.edge_schedule(P, N_EPOCHS)
+    pairs = np.asarray(R.mid_near_pairs_dense(X, 5, 6, int(seed), int(n_threads)))
+    Y0 = pca_init(X, seed)
+    return dict(X=X, labels=labels, P=P, head=head, tail=tail, eps=eps, pairs=pairs, Y0=Y0, n=n,
+                setup_s=time.time() - t0, graph="the reference's NN-descent") | pass_params(n, seed)
 
 
 def sgd_args(w, n_epochs=N_EPOCHS, mid_w=MID_W):
     mid_len = max(1.0, 0.5 * n_epochs)
     return dict(e0=0, e1=n_epochs, alpha0=1.0, alpha1=0.0, mid0=mid_w, mid1=mid_w * max(0.0, 1.0 - n_epochs / mid_len))
+
+
+# ----------------------------------------------------------------------------------------------- configs 1, 2, 4
+def config1_data(n=10_000, d=50, centres=10, seed=0):
+    """the loss="umap" configuration's data: ten centres N(0, 5^2 I), labels uniform, X = centre + N(0, I), from
+    default_rng(seed) in that order"""
+    rng = np.random.default_rng(seed)
+    C = rng.normal(0, 5.0, (centres, d))
+    y = rng.integers(0, centres, n)
+    return (C[y] + rng.normal(0, 1, (n, d))).astype(np.float32), y
+
+
+def config2_data(n=70_000, classes=10, seed=1):
+    """the loss="tsne" configuration's data, image-like rows of 28 x 28 pixels: ten class prototypes, each with 149
+    of the 400 pixels of the centred 20 x 20 block (about 19 % of the image) drawn U[0, 1] and the rest 0; a row is
+    its class's prototype plus N(0, 0.1^2) per pixel, clipped to [0, 1]; default_rng(seed)"""
+    rng = np.random.default_rng(seed)
+    block = np.array([r * 28 + c for r in range(4, 24) for c in range(4, 24)])
+    protos = np.zeros((classes, 784), np.float32)
+    for k in range(classes):
+        px = rng.choice(block, 149, replace=False)
+        protos[k, px] = rng.uniform(0, 1, 149)
+    y = rng.integers(0, classes, n)
+    X = np.empty((n, 784), np.float32)
+    for s in range(0, n, 10_000):
+        e = min(n, s + 10_000)
+        X[s:e] = np.clip(protos[y[s:e]] + rng.normal(0, 0.1, (e - s, 784)), 0.0, 1.0)
+    return X, y
+
+
+def config4_instances(count=256, d=32):
+    """the batched configuration's layouts: instance i (seed 100 + i) has n = round(exp(U[ln 500, ln 20000])) points
+    in d = 32 from a mixture of 3-20 Gaussians (centres N(0, 6^2 I), equal weights, unit covariance)"""
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng(100 + i)
+        n = int(round(np.exp(rng.uniform(np.log(500.0), np.log(20000.0)))))
+        k = int(rng.integers(3, 21))
+        C = rng.normal(0, 6.0, (k, d))
+        out.append((C[rng.integers(0, k, n)] + rng.normal(0, 1, (n, d))).astype(np.float32))
+    return out
+
+
+def perplexity_affinities(ind, d2, perplexity=30.0, n_steps=100, tol=1e-5):
+    """t-SNE's input affinities, which the reference does not build (its t-SNE pass takes the fuzzy graph): per row,
+    p_j|i = exp(-beta_i d2_ij) / sum_j exp(-beta_i d2_ij) over the row's neighbours (squared distances d2), with beta_i
+    bisected until the row's entropy is log(perplexity) nats within tol (at most n_steps: double or halve beta until
+    the target is bracketed, then halve the bracket), in FP64; then P = (P_cond + P_cond^T) / (2 n), CSR float32"""
+    import scipy.sparse as sp
+    d2 = np.asarray(d2, dtype=np.float64)
+    n, k = d2.shape
+    target = np.log(perplexity)
+    beta = np.ones(n)
+    lo = np.full(n, -np.inf)
+    hi = np.full(n, np.inf)
+    active = np.ones(n, bool)
+    p = np.empty_like(d2)
+    for _ in range(n_steps):
+        idx = np.flatnonzero(active)
+        if idx.size == 0:
+            break
+        e = np.exp(-d2[idx] * beta[idx, None])
+        s = np.maximum(e.sum(1), 1e-8)
+        H = np.log(s) + beta[idx] * (d2[idx] * e).sum(1) / s
+        p[idx] = e / s[:, None]
+        diff = H - target
+        ok = np.abs(diff) <= tol
+        active[idx[ok]] = False
+        up = idx[(diff > 0) & ~ok]
+        dn = idx[(diff <= 0) & ~ok]
+        lo[up] = beta[up]
+        beta[up] = np.where(np.isinf(hi[up]), beta[up] * 2.0, (beta[up] + hi[up]) / 2.0)
+        hi[dn] = beta[dn]
+        beta[dn] = np.where(np.isinf(lo[dn]), beta[dn] / 2.0, (beta[dn] + lo[dn]) / 2.0)
+    rows = np.repeat(np.arange(n), k)
+    C = sp.csr_matrix((p.ravel(), (rows, np.asarray(ind).ravel())), shape=(n, n))
+    P = ((C + C.T) / (2.0 * n)).tocsr().astype(np.float32)
+    P.sort_indices()
+    return P
+
+
+def kl_divergence(P, Y, dof=1.0, block=4096):
+    """KL(P || Q) of a layout, Q the Student-t similarities normalised over all pairs i != j (FP64, blocked)"""
+    import scipy.sparse as sp
+    P = sp.csr_matrix(P, dtype=np.float64)
+    P = P / P.sum()
+    Y = np.asarray(Y, dtype=np.float64)
+    n = Y.shape[0]
+    Z = 0.0
+    for s in range(0, n, block):
+        d2 = ((Y[s:s + block, None, :] - Y[None, :, :]) ** 2).sum(-1)
+        w = (1.0 + d2 / dof) ** (-dof)
+        w[np.arange(w.shape[0]), np.arange(s, s + w.shape[0])] = 0.0
+        Z += w.sum()
+    C = P.tocoo()
+    q = (1.0 + ((Y[C.row] - Y[C.col]) ** 2).sum(-1) / dof) ** (-dof) / Z
+    return float((C.data * np.log(C.data / q)).sum())
+
+
+def exact_knn_cpu(X, k):
+    """(indices (n, k), squared distances (n, k)) of the k nearest other rows, exact, on the host's cores"""
+    from sklearn.neighbors import NearestNeighbors
+    d, i = NearestNeighbors(n_neighbors=k + 1, algorithm="brute", n_jobs=-1).fit(X).kneighbors(X)
+    return i[:, 1:].astype(np.int64), (d[:, 1:].astype(np.float64) ** 2)
+
+
+def config_leg(cfg, impl, steps, warmup):
+    """one JSON line for configuration 1 (10k umap SGD, 500 epochs, n_threads = 1) or 2 (70k tsne, perplexity 30,
+    750 iterations with 250 of early exaggeration 12): the layout pass's seconds per layout with device-resident
+    inputs (for configuration 1 the serial stream mode, the reference's single stream, and the counter mode beside
+    it), or the reference's CPU path (impl "reference"), with 15-NN preservation and KL of the result"""
+    nt = os.cpu_count() or 1
+    if cfg == 1:
+        import scipy.sparse as sp
+        g = dict(np.load(os.path.join(ROOT, "tests", "golden", "layout_config1.npz")))
+        X, _ = config1_data()
+        P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(X.shape[0],) * 2)
+        n_epochs, seed = int(g["n_epochs"]), int(g["seed"])
+        config = {"workload": "umap layout, n=10000, d=50, 10 Gaussians, seed 0, k=15 (the reference's NN-descent "
+                              "graph and spectral init, captured from its fit), 500 epochs, n_threads=1",
+                  "n_points": 10000, "l2": "inputs in L2 (6 MB of edges); no flush between epochs, as in a layout pass"}
+        out = {"metric": "10k umap layout s (500 epochs, n_threads=1)", "unit": "s", "steps": steps,
+               "warmup": warmup, "higher_is_better": False, "dtype": "f32", "data": "synthetic", "config": config}
+        if impl == "reference":
+            from oracle import oracle as O
+            head, tail, eps = O.edge_schedule(P, n_epochs)
+            times, Y = [], None
+            for i in range(warmup + steps):
+                Y = g["Y0"].copy()
+                t0 = time.perf_counter()
+                O.optimize_sgd(Y, head, tail, eps, n_epochs, mid_weight=float(g["mid_w"]), mid_pairs=g["mid_pairs"],
+                               backend="reference", n_threads=1, seed=seed, a=float(g["a"]), b=float(g["b"]),
+                               rep_a=float(g["rep_a"]), rep_b=float(g["rep_b"]), indptr=P.indptr, indices=P.indices)
+                if i >= warmup:
+                    times.append(time.perf_counter() - t0)
+            out |= {"impl": "reference", "cores": 1, "value": round(statistics.median(times), 4),
+                    "knn15": round(knn_preservation(X, Y), 4), "kl": round(kl_divergence(P, Y), 4)}
+        else:
+            import torch
+            import magnet_b200 as mg
+            head, tail, eps = mg.edge_schedule(P, n_epochs)
+            dev = torch.device("cuda", torch.cuda.current_device())
+            t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+            hd, td, ed, pd = t(head), t(tail), t(eps), t(g["mid_pairs"])
+            ipd, ixd = t(P.indptr.astype(np.int32)), t(P.indices.astype(np.int32))
+            Y0 = t(g["Y0"])
+            eonns0 = (ed / 5.0).contiguous()
+            z, zf = torch.zeros(0, dtype=torch.int32, device=dev), torch.zeros(0, dtype=torch.float32, device=dev)
+            z2 = torch.zeros((0, 2), dtype=torch.float32, device=dev)
+
+            def run(mode):
+                # MAGNET._optimize's one call over [0, 500): alpha 1 -> 0, mid weight mid_w -> 0 (its window is 250
+                # epochs, so it reaches 0 at the end of the call)
+                Y, eons, eonns = Y0.clone(), ed.clone(), eonns0.clone()
+                mg.optimize_layout(Y, hd, td, ed, eons, eonns, ipd, ixd, 0, n_epochs, 1.0, 0.0, float(g["mid_w"]), 0.0,
+                                   float(g["a"]), float(g["b"]), float(g["rep_a"]), float(g["rep_b"]), 5.0, 0, 1.0,
+                                   2.0, 4, 0.25, 0, 0, 0, z2, z2, z, 0.9, 0.999, z, pd, z, z, 0.0, 0, zf, seed, -1, 0,
+                                   None, None, 1 if mode == "serial" else 0)
+                return Y
+            for mode in ("serial", "hogwild"):
+                for _ in range(warmup):
+                    run(mode)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(steps):
+                    Y = run(mode)
+                e1.record()
+                torch.cuda.synchronize()
+                Yh = Y.cpu().numpy()
+                out[mode] = {"value": round(e0.elapsed_time(e1) / steps / 1000, 4),
+                             "knn15": round(knn_preservation(X, Yh), 4), "kl": round(kl_divergence(P, Yh), 4)}
+            out["value"] = out["serial"]["value"]
+        print(json.dumps(out))
+        return
+    # configuration 2
+    X, _ = config2_data()
+    n = X.shape[0]
+    t0 = time.time()
+    if impl == "reference":
+        ind, d2 = exact_knn_cpu(X, 90)
+    else:
+        from magnet_b200 import graph as G
+        ind, dist = G.exact_knn(X, 91)
+        d2 = dist.astype(np.float64) ** 2
+    P = perplexity_affinities(ind, d2, 30.0)
+    Y0 = pca_init(X, 1)
+    Y0 = np.ascontiguousarray(Y0 / max(float(Y0[:, 0].std()), 1e-12) * 1e-4, dtype=np.float32)
+    setup_s = time.time() - t0
+    config = {"workload": "tsne layout, n=70000, d=784 image-like rows (10 prototypes), seed 1, perplexity 30 "
+                          "(90 neighbours), 750 iterations with 250 of early exaggeration 12, 3 points per box",
+              "n_points": n, "l2": "inputs larger than L2 for the affinities (%d MB)" % (P.nnz * 8 // 2 ** 20)}
+    if impl == "reference":
+        from oracle import oracle as O
+        for _ in range(warmup):
+            O.TsneRun(P, Y0.copy(), n_iter=1, early_iter=1, n_threads=-1, backend="reference").advance(1)
+        run = O.TsneRun(P, Y0.copy(), n_iter=750, early_iter=250, n_threads=-1, backend="reference")
+        times = []
+        for k in split_iterations(750, steps):
+            t1 = time.perf_counter()
+            run.advance(k)
+            times.append(time.perf_counter() - t1)
+        Y = run.Y
+        line = {"impl": "reference", "cores": nt, "value": round(sum(times), 3),
+                "sample": "the whole 750 iterations timed in %d consecutive pieces" % steps}
+    else:
+        import torch
+        import magnet_b200 as mg
+        dev = torch.device("cuda", torch.cuda.current_device())
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        Pn = P / P.sum()
+        ipd, ixd, dd = t(Pn.indptr.astype(np.int32)), t(Pn.indices.astype(np.int32)), t(Pn.data.astype(np.float32))
+        Yd0 = t(Y0)
+        Yd = torch.empty_like(Yd0)
+
+        def run():
+            Yd.copy_(Yd0)
+            mg._native.optimize_tsne(ipd, ixd, dd, Yd, 750, 250, 12.0, 1.0, -1.0, 0.5, 0.8, 3, 0.7, 1.0, 20, 1000, 0,
+                                     True)
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        Y = Yd.cpu().numpy()
+        line = {"value": round(e0.elapsed_time(e1) / steps / 1000, 4)}
+    out = {"metric": "70k tsne layout s (750 iterations)", "unit": "s", "steps": steps, "warmup": warmup,
+           "higher_is_better": False, "dtype": "f32", "data": "synthetic", "config": config,
+           "inputs": {"knn": "exact, on the host's cores" if impl == "reference" else "exact, on the device",
+                      "nnz": int(P.nnz), "setup_s": round(setup_s, 1)},
+           "knn15": round(knn_preservation(X, Y), 4), "kl": round(kl_divergence(P, Y), 4)} | line
+    print(json.dumps(out))
+
+
+def config4_leg(impl, steps, warmup, count=256, n_iter=500):
+    """the batched form: `count` independent perplexity-30 t-SNE layouts of 500-20,000 points, 500 iterations each
+    (166 of early exaggeration 12, MAGNET's default min(250, n_iter // 3) for loss="tsne"); layouts/s of the batch
+    (one CUDA graph per iteration, the layouts as branches, launch shapes from the autotuner) beside the plain device
+    form (one optimize_tsne call per layout, in sequence), or the reference's loop of optimize_tsne calls on the
+    host's cores over a size-stratified sample of the layouts (impl "reference"); per-layout KL and 15-NN on the
+    sample"""
+    Xs = config4_instances(count)
+    early = min(250, n_iter // 3)
+    sample = sorted(range(count), key=lambda i: Xs[i].shape[0])[::16]
+    t0 = time.time()
+    Ps, Y0s = [], []
+    for i, X in enumerate(Xs):
+        if impl == "reference":
+            ind, d2 = exact_knn_cpu(X, 90)
+        else:
+            from magnet_b200 import graph as G
+            ind, dist = G.exact_knn(X, 91)
+            d2 = dist.astype(np.float64) ** 2
+        Ps.append(perplexity_affinities(ind, d2, 30.0))
+        Y0 = pca_init(X, 100 + i)
+        Y0s.append(np.ascontiguousarray(Y0 / max(float(Y0[:, 0].std()), 1e-12) * 1e-4, dtype=np.float32))
+    setup_s = time.time() - t0
+    config = {"workload": "%d t-SNE layouts, n log-uniform in [500, 20000] (total %d), d=32, 3-20 Gaussians each, "
+                          "seeds 100-%d, perplexity 30, %d iterations (%d early)" % (count, sum(len(X) for X in Xs),
+                                                                                    99 + count, n_iter, early),
+              "n_layouts": count}
+
+    def quality_of(Ys):
+        return {"kl": [round(kl_divergence(Ps[i], Ys[i]), 4) for i in sample],
+                "knn15": [round(knn_preservation(Xs[i], Ys[i]), 4) for i in sample]}
+    if impl == "reference":
+        from oracle import oracle as O
+        times, Ys = [], {}
+        for i in sample:
+            t1 = time.perf_counter()
+            Ys[i] = O.optimize_tsne(Ps[i], Y0s[i].copy(), n_iter=n_iter, early_iter=early, n_threads=-1,
+                                    backend="reference")
+            times.append(time.perf_counter() - t1)
+        out = {"impl": "reference", "value": round(len(sample) / sum(times), 4), "cores": os.cpu_count(),
+               "sample": "%d of the %d layouts (every 16th by size), each a whole optimize_tsne pass" % (len(sample),
+                                                                                                        count),
+               "per_layout_s": [round(t, 3) for t in times], "quality": quality_of(Ys)}
+    else:
+        import torch
+        import magnet_b200 as mg
+        from magnet_b200 import autotune as A
+        Ys = [Y.copy() for Y in Y0s]
+        mg.optimize_tsne_batch(Ps, Ys, n_iter=n_iter, early_iter=early)     # tunes once for this shape (cached)
+        key = A.batch_key([len(X) for X in Xs], [P.nnz for P in Ps])
+        choice = A.lookup(key) or {}
+        graphs = [(P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data.astype(np.float32)) for P in Ps]
+        batch = mg._native.TsneBatch(graphs, n_iter=n_iter, early_iter=early,
+                                     threads_per_row=int(choice.get("threads_per_row", 0)),
+                                     branches=int(choice.get("branches", 32)))
+        dev = torch.device("cuda", torch.cuda.current_device())
+        Yd0 = [torch.from_numpy(Y).to(dev) for Y in Y0s]
+        Yd = [torch.empty_like(Y) for Y in Yd0]
+        for _ in range(warmup):
+            for a, b in zip(Yd, Yd0):
+                a.copy_(b)
+            batch.run(Yd)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(steps):
+            for a, b in zip(Yd, Yd0):
+                a.copy_(b)
+            batch.run(Yd)
+        torch.cuda.synchronize()
+        batched_s = (time.perf_counter() - t1) / steps
+        Yb = [Y.cpu().numpy() for Y in Yd]
+        t1 = time.perf_counter()
+        for a, b, G_ in zip(Yd, Yd0, graphs):
+            a.copy_(b)
+            mg._native.optimize_tsne(G_[0], G_[1], G_[2], a, n_iter, early, 12.0, 1.0, -1.0, 0.5, 0.8, 3, 0.7, 1.0,
+                                     20, 1000, int(choice.get("threads_per_row", 0)), True)
+        torch.cuda.synchronize()
+        plain_s = time.perf_counter() - t1
+        out = {"value": round(count / batched_s, 3), "batched_s": round(batched_s, 3),
+               "plain": {"value": round(count / plain_s, 3), "s": round(plain_s, 3)},
+               "speedup_vs_plain": round(plain_s / batched_s, 2), "autotune": choice,
+               "kernels_per_iteration": int(batch.kernels_per_iteration), "quality": quality_of(Yb)}
+    line = {"metric": "batched t-SNE layouts/s (256 layouts, 500 iterations)", "unit": "layouts/s",
+            "higher_is_better": True, "steps": steps, "warmup": warmup, "dtype": "f32", "data": "synthetic",
+            "config": config, "inputs": {"setup_s": round(setup_s, 1), "sample": sample}} | out
+    print(json.dumps(line))
 
 
 # ----------------------------------------------------------------------------------------------- GPU arm
@@ -153,6 +542,69 @@ class GpuPass:
 
 
 # ----------------------------------------------------------------------------------------------- reference CPU path
+def reference_sgd(R, w, Y, eons, eonns, e0, e1, n_threads):
+    """one optimize_layout call of the reference over epochs [e0, e1) with the pass's linear schedules (as
+    MAGNET._optimize makes them, magnet/__init__.py:796-839)"""
+    z = np.zeros(0, np.int32)
+    alpha = lambda e: 1.0 - e / N_EPOCHS
+    mid = lambda e: MID_W * (1.0 - e / N_EPOCHS)   # the single call's linear interpolation of sgd_args
+    R.optimize_layout(Y, w["head"], w["tail"], w["eps"], eons, eonns, z, z, e0, e1, alpha(e0), alpha(e1), mid(e0),
+                      mid(e1), w["a"], w["b"], w["rep_a"], w["rep_b"], 5.0, 0, 1.0, 2.0, 4, 0.25, 0, 0, 0,
+                      np.zeros((0, 2), np.float32), np.zeros((0, 2), np.float32), z, 0.9, 0.999, z, w["pairs"], z, z,
+                      0.0, 0, np.zeros(0, np.float32), w["seed"], n_threads, 0)
+
+
+def rescale(Y, n):
+    """the hybrid pass's recentre + rescale to std 31 sqrt(n / 70000) (magnet/__init__.py:695-696)"""
+    Y -= Y.mean(0)
+    Y *= np.float32(31.0 * np.sqrt(n / 70000.0) / max(float(Y[:, 0].std()), 1e-12))
+    return Y
+
+
+def split_iterations(total, pieces):
+    """total iterations in `pieces` near-equal consecutive runs"""
+    return [total // pieces + (1 if j < total % pieces else 0) for j in range(pieces)] if pieces > 0 else []
+
+
+class ReferencePass:
+    """The whole hybrid pass on the reference's CPU path (its compiled module on all host threads, driven as
+    MAGNET.fit drives it for loss="hybrid", magnet/__init__.py:683-700), cut into `pieces` consecutive timed
+    pieces: piece 0 is the SGD pass (one optimize_layout call of 200 epochs, as the reference makes it) and the
+    rescale, pieces 1.. are the 300 full-batch iterations in near-equal runs of the reference's t-SNE loop
+    (magnet/tsne.py:132-184, the loop restated in oracle.TsneRun, state carried from piece to piece). The pieces
+    together run one whole pass; their times add up to the seconds per layout."""
+
+    def __init__(self, w, pieces, n_threads):
+        from oracle import oracle as O
+        self.O, self.R, self.w, self.nt = O, O.reference(), w, n_threads
+        self.pieces = max(1, int(pieces))
+        self.iters = split_iterations(HYBRID_ITER, self.pieces - 1)
+        self.Y = self.run = None
+
+    def piece(self, j):
+        w = self.w
+        if j == 0:
+            self.Y = w["Y0"].copy()
+            eons, eonns = w["eps"].copy(), (w["eps"] / np.float32(5.0)).astype(np.float32)
+            reference_sgd(self.R, w, self.Y, eons, eonns, 0, N_EPOCHS, self.nt)
+            rescale(self.Y, w["n"])
+            self.run = self.O.TsneRun(w["P"], self.Y, n_iter=HYBRID_ITER, early_iter=0, exaggeration=1.0,
+                                      n_threads=self.nt, backend="reference")
+            if self.pieces == 1:
+                self.run.advance(HYBRID_ITER)
+        else:
+            self.run.advance(self.iters[j - 1])
+        return self.run.Y
+
+    def warmup(self):
+        """one SGD epoch and one iteration on copies (pages in the inputs and the module)"""
+        w = self.w
+        Y = w["Y0"].copy()
+        reference_sgd(self.R, w, Y, w["eps"].copy(), (w["eps"] / np.float32(5.0)).astype(np.float32), 0, 1, self.nt)
+        self.O.TsneRun(w["P"], rescale(Y, w["n"]), n_iter=1, early_iter=0, n_threads=self.nt,
+                       backend="reference").advance(1)
+
+
 def reference_sample(w, Y_tsne=None, sgd_epochs=2, tsne_iters=2):
     """The reference's CPU implementation (its compiled module, all host threads) on a bounded sample: SGD epochs
     at mid-run sampling density and full-batch iterations of the hybrid pass; returns seconds per whole layout
@@ -170,24 +622,15 @@ def reference_sample(w, Y_tsne=None, sgd_epochs=2, tsne_iters=2):
     e_mid = N_EPOCHS // 2
     eons0 = (e_mid + rng.uniform(0, 1, eps.size).astype(np.float32) * eps).astype(np.float32)
     eonns0 = (eons0 - eps / 5.0).astype(np.float32)
-    z = np.zeros(0, np.int32)
-    alpha = lambda e: 1.0 - e / N_EPOCHS
-    mid = lambda e: MID_W * max(0.0, 1.0 - e / (0.5 * N_EPOCHS))
 
     def sgd(k):
         Y, eons, eonns = w["Y0"].copy(), eons0.copy(), eonns0.copy()
         t0 = time.perf_counter()
-        R.optimize_layout(Y, w["head"], w["tail"], eps, eons, eonns, z, z, e_mid, e_mid + k, alpha(e_mid),
-                          alpha(e_mid + k), mid(e_mid), mid(e_mid + k), w["a"], w["b"], w["rep_a"],
-                          w["rep_b"], 5.0, 0, 1.0, 2.0, 4, 0.25, 0, 0, 0, np.zeros((0, 2), np.float32),
-                          np.zeros((0, 2), np.float32), z, 0.9, 0.999, z, w["pairs"], z, z, 0.0, 0,
-                          np.zeros(0, np.float32), w["seed"], nt, 0)
+        reference_sgd(R, w, Y, eons, eonns, e_mid, e_mid + k, nt)
         return time.perf_counter() - t0
 
     if Y_tsne is None:
-        Y_tsne = w["Y0"].copy()
-        Y_tsne -= Y_tsne.mean(0)
-        Y_tsne *= np.float32(31.0 * np.sqrt(n / 70000.0) / max(float(Y_tsne[:, 0].std()), 1e-12))
+        Y_tsne = rescale(w["Y0"].copy(), n)
 
     def tsne(k):
         t0 = time.perf_counter()
@@ -252,31 +695,29 @@ class Clocks:
 
 
 def knn_preservation(X, Y, k=15, n_query=5000, seed=0):
-    """15-NN preservation of benchmarks/metrics.py: exact k-NN of a query subsample in the data and in the layout,
-    mean overlap / k (torch on the device)"""
-    import torch
-    dev = torch.device("cuda", torch.cuda.current_device())
+    """15-NN preservation of benchmarks/metrics.py:52-62: the exact k-NN of a seeded 5,000-row query subsample in
+    the data and in the layout, mean overlap / k. Computed on the host's cores (brute force in the data, a k-d tree
+    in the layout) with the same code in both arms, so the two figures compare like with like."""
+    from sklearn.neighbors import NearestNeighbors
+    from scipy.spatial import cKDTree
     rng = np.random.default_rng(seed)
-    q = rng.choice(X.shape[0], min(n_query, X.shape[0]), replace=False)
+    q = np.sort(rng.choice(X.shape[0], min(n_query, X.shape[0]), replace=False))
+    hi = NearestNeighbors(n_neighbors=k + 1, algorithm="brute", n_jobs=-1).fit(X).kneighbors(
+        X[q], return_distance=False)
+    Yd = np.asarray(Y, dtype=np.float64)
+    lo = cKDTree(Yd).query(Yd[q], k + 1, workers=-1)[1]
 
-    def knn(A):
-        A = torch.from_numpy(np.ascontiguousarray(A, dtype=np.float32)).to(dev)
-        sq = (A * A).sum(1)
-        out = []
-        for s in range(0, len(q), 1024):
-            idx = torch.from_numpy(q[s:s + 1024]).to(dev)
-            d = sq[idx, None] - 2 * A[idx] @ A.T + sq[None]
-            d[torch.arange(len(idx), device=dev), idx] = float("inf")
-            out.append(torch.topk(d, k, largest=False).indices.cpu().numpy())
-        return np.concatenate(out)
-    a, b = knn(X), knn(Y)
+    def drop_self(rows):
+        return [[j for j in r if j != i][:k] for i, r in zip(q, rows)]
+    a, b = drop_self(hi), drop_self(lo)
     return float(np.mean([len(np.intersect1d(a[i], b[i])) / k for i in range(len(q))]))
 
 
-def roofline(w, gp, peaks):
+def roofline(w, gp, peak):
     """per-stage CUDA-event times of the t-SNE iteration and of the SGD epoch kernel, the dominant kernel's
     achieved GB/s against its algorithmic bytes"""
     import torch
+    peaks, peak_src = peak
     mg = gp.mg
     d = gp.d
     n = w["n"]
@@ -324,7 +765,7 @@ def roofline(w, gp, peaks):
                      "unit": "GB/s", "frac": round(achieved / peaks, 4),
                      "traffic": None if traffic is None else round(traffic, 0),
                      "alg_bytes_per_launch": alg[dom], "launch_ms": round(ms, 4),
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "peak_source": peak_src},
         "stages_ms": {k: round(v, 4) for k, v in stages.items()} | {"sgd_epoch": round(sgd_ms, 4)},
         "step_share_ms": {k: round(v, 2) for k, v in share.items()},
         "fft_pass": {"alg_bytes": fft_pass_bytes, "ms": round(fft_pass_ms, 4),
@@ -351,11 +792,13 @@ def measured_traffic(stage, n):
 
 
 def measured_peak():
+    """(HBM GB/s, where it came from): the pool's measured copy bandwidth when MEASURED_PEAKS.json is present, else
+    the earlier measurement of this pool's B200s (6,650 GB/s)"""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["hbm_gbs"])
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
     except (OSError, KeyError, ValueError):
-        return 6650.0
+        return 6650.0, "6650 GB/s, an earlier copy measurement on this pool (of fallback)"
 
 
 # ----------------------------------------------------------------------------------------------- fuzzy graph
@@ -600,7 +1043,19 @@ def main():
     ap.add_argument("--graph", action="store_true", help="time the fuzzy neighbour graph instead of the layout")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4],
+                    help="1: the 10k umap layout, 2: the 70k tsne layout, 3 (default): the 1M hybrid layout, "
+                         "4: 256 batched t-SNE layouts")
     args = ap.parse_args()
+    if args.config in (1, 2, 4):
+        if args.impl != "reference":
+            import torch
+            torch.cuda.set_device(0)
+        if args.config == 4:
+            config4_leg(args.impl, args.steps, args.warmup)
+        else:
+            config_leg(args.config, args.impl, args.steps, args.warmup)
+        return
     if args.graph:
         import torch
         torch.cuda.set_device(0)
@@ -610,6 +1065,51 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the same config in both arms (the graph each arm builds is named in "inputs")
+    config = {"workload": "hybrid layout, n=%d, d=50, 100 anisotropic Gaussians, seed 2, k=15, %d SGD epochs + %d "
+                          "FFT iterations" % (args.n, N_EPOCHS, HYBRID_ITER),
+              "n_points": args.n, "l2": "inputs larger than L2 (126 MB): about 24 edges per point, 20 B each",
+              "init": "PCA (spectral stand-in)", "parallelism": "replicas %d" % world}
+
+    if args.impl == "reference":
+        # the reference's CPU path needs no GPU and no process group: rank 0 alone runs it, the others exit
+        if rank != 0:
+            return
+        nt = os.cpu_count() or 1
+        w = make_workload_reference(args.n, n_threads=-1)
+        rp = ReferencePass(w, args.steps, -1)
+        for _ in range(args.warmup):
+            rp.warmup()
+        times = []
+        Y_ref = None
+        for j in range(args.steps):
+            t0 = time.perf_counter()
+            Y_ref = rp.piece(j)
+            times.append(time.perf_counter() - t0)
+        value = sum(times)
+        knn15 = knn_preservation(w["X"], Y_ref)
+        sample = ("the whole pass, timed in %d consecutive pieces: piece 1 the 200-epoch SGD call and the rescale "
+                  "(%.2f s), pieces 2-%d the 300 full-batch iterations (%.2f s); the reference's compiled module on "
+                  "all %d host threads" % (args.steps, times[0], args.steps, sum(times[1:]), nt)) \
+            if args.steps > 1 else "the whole pass in one step on all %d host threads" % nt
+        line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value * 1000 / args.steps, 1),
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": config,
+                "inputs": {"graph": w["graph"], "edges": int(w["head"].size), "setup_s": round(w["setup_s"], 1)},
+                "knn15": round(knn15, 4),
+                "pass_s": {"sgd_and_rescale": round(times[0], 3), "tsne": round(sum(times[1:]), 3)},
+                "cpu_baseline": {"value": round(value, 3), "unit": "s", "cores": nt, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": round(value, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if not args.no_serve:
+            try:
+                line.update(reference_serve(n_requests=args.serve_requests))
+            except Exception as e:  # noqa: BLE001  (the layout's line is reported either way)
+                line["transform"] = {"error": "%s: %s" % (type(e).__name__, e)}
+        print(json.dumps(line))
+        return
+
     import torch
     dist = None
     if world > 1:
@@ -620,46 +1120,8 @@ def main():
     else:
         torch.cuda.set_device(0)
 
-    config = {"workload": "hybrid layout, n=%d, d=50, 100 anisotropic Gaussians, seed 2, k=15, %d SGD epochs + %d "
-                          "FFT iterations" % (args.n, N_EPOCHS, HYBRID_ITER),
-              "n_points": args.n, "l2": "inputs larger than L2 (graph ~%d MB)" % 0, "init": "PCA (spectral stand-in)"}
-
-    if args.impl == "reference":
-        if rank != 0:
-            if dist is not None:
-                dist.destroy_process_group()
-            return
-        w = make_workload(args.n)
-        config["l2"] = "inputs larger than L2 (edge arrays %d MB)" % (w["head"].nbytes * 5 // 2 ** 20)
-        vals = []
-        nt = os.cpu_count() or 1
-        sample = ""
-        for i in range(args.warmup + args.steps):
-            v, nt, sample = reference_sample(w, sgd_epochs=3, tsne_iters=3)
-            if i >= args.warmup:
-                vals.append(v)
-        value = statistics.mean(vals)
-        line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value * 1000, 1),
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": round(value, 3), "unit": "s", "cores": nt, "kind": "reference",
-                                 "sample": "per step: " + sample},
-                "e2e": {"value": round(value, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        if not args.no_serve:
-            try:
-                line.update(reference_serve(n_requests=args.serve_requests))
-            except Exception as e:  # noqa: BLE001  (the layout's line is reported either way)
-                line["transform"] = {"error": "%s: %s" % (type(e).__name__, e)}
-        if dist is not None:
-            dist.destroy_process_group()
-        print(json.dumps(line))
-        return
-
     import magnet_b200 as mg
     w = make_workload(args.n)
-    config["l2"] = "inputs larger than L2 (edge arrays %d MB)" % (w["head"].nbytes * 5 // 2 ** 20)
-    config["setup_s"] = round(w["setup_s"], 1)
     gp = GpuPass(w)
     for _ in range(args.warmup):
         gp.step_device()
@@ -691,14 +1153,15 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / max(1, min(args.steps, 3)), dist, "cuda")
 
-    peaks = measured_peak()
-    rf = roofline(w, gp, peaks)
+    rf = roofline(w, gp, measured_peak())
     knn15 = knn_preservation(w["X"], Y_final)
     n_gpus = world
     line = {"metric": METRIC, "value": round(seconds_per_layout(ms, n_gpus), 4), "unit": "s", "n_gpus": n_gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config | {"knn15": round(knn15, 4), "grid": rf["grid"], "parallelism": "replicas %d" % n_gpus},
+            "config": config,
+            "inputs": {"graph": w["graph"], "edges": int(w["head"].size), "setup_s": round(w["setup_s"], 1)},
+            "knn15": round(knn15, 4), "grid": rf["grid"],
             "e2e": {"value": round(seconds_per_layout(e2e_ms, n_gpus), 4), "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": rf["roofline"],

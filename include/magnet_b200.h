@@ -127,6 +127,26 @@ int mg_optimize_tsne(const int32_t* indptr, const int32_t* indices, const float*
  * 8 all; grid[4] receives the last iteration's (n_boxes, N, M, Mh). */
 int mg_optimize_tsne_profiled(const int32_t* indptr, const int32_t* indices, const float* P, int64_t n, int64_t nnz,
                               float* Y, const mg_tsne_params* p, double* stage_ms, int* grid);
+/* ================================================================ batched t-SNE layouts
+ * Many independent optimize_tsne passes (magnet/tsne.py:132-214; the reference runs them as a loop of
+ * optimize_tsne calls) of uneven size, run together: each layout keeps its own device state, and one CUDA graph
+ * holds one iteration of every layout as independent branches (layout i on branch i mod `branches`), replayed
+ * once per iteration. Every layout uses the same parameters p (n_iter, early_iter, schedule, n_interp, box width);
+ * its grid is allocated for max_boxes[i] boxes per side (NULL: 64 + 2 ceil(sqrt(n_i)) rounded up to a multiple of
+ * 4, capped by p->max_boxes), and a layout that outgrows it is clamped to that many boxes (wider boxes). The
+ * arrays of layout i are indptr[i] (n[i] + 1), indices[i] / P[i] (nnz[i]), host or device; P is normalised to
+ * sum 1 inside. */
+typedef struct mg_tsne_batch mg_tsne_batch;
+int mg_tsne_batch_create(int count, const int64_t* n, const int64_t* nnz, const int32_t* const* indptr,
+                         const int32_t* const* indices, const float* const* P, const mg_tsne_params* p,
+                         const int* max_boxes, int branches, mg_tsne_batch** out);
+/* Runs p->n_iter iterations of every layout from Y[i] ((n[i], 2), host or device), updated in place. Synchronous.
+ * The first run on a stream captures the iteration graph. */
+int mg_tsne_batch_run(mg_tsne_batch* b, float* const* Y);
+/* Layout count and kernels per replayed iteration (0 before the first run). */
+int mg_tsne_batch_size(const mg_tsne_batch* b, int* count, uint64_t* kernels_per_iteration);
+void mg_tsne_batch_destroy(mg_tsne_batch* b);
+
 /* Hybrid hand-off (magnet/__init__.py:695-696): Y (n, dim) -= column means, then Y *= target_std / std(Y[:, 0]). */
 int mg_center_scale(float* Y, int64_t n, int dim, double target_std);
 

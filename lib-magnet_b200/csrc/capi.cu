@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 #include <thread>
+#include <functional>
 
 namespace mgb {
 
@@ -50,6 +51,12 @@ int guard(F&& f) {
     }
 }
 
+}  // namespace
+
+// the C-ABI convention for entry points defined in other files: status code and the thread's last error
+int guard_call(const std::function<void()>& f) { return guard(f); }
+
+namespace {
 // device view of a caller array: the pointer itself when it is device memory, else a staged copy
 template <class T>
 T* in_dev(const T* p, int64_t count, int slot, cudaStream_t s) {

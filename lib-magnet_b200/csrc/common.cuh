@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <string>
 #include <stdexcept>
+#include <functional>
 
 #include "../../include/magnet_b200.h"
 
@@ -120,5 +121,8 @@ inline bool is_device_ptr(const void* ptr) {
 
 // Current stream of the calling host thread (mg_set_stream).
 cudaStream_t current_stream();
+
+// Runs f with the C ABI's error convention: MG_OK, or the error's code with its message kept for mg_last_error().
+int guard_call(const std::function<void()>& f);
 
 }  // namespace mgb

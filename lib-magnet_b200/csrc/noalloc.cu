@@ -19,7 +19,8 @@ namespace {
 
 constexpr int kNoallocMaxM = 512;                           // largest FFT side (so N = n_boxes * n_interp <= 512)
 constexpr int kMh = kNoallocMaxM / 2 + 1;                   // half-spectrum columns
-constexpr int kNp = kNoallocMaxM + (kNoallocMaxM & 1);      // row pairs, padded to even
+constexpr int kNp = (kNoallocMaxM + 3) & ~3;                // rows rounded up to 4, as RepBuffers::alloc rounds
+static_assert(kNp % 4 == 0, "the transposed spectra are written in 32-byte groups of 4 rows");
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // scratch layout (byte offsets), the same buffers RepBuffers holds for Nmax = Mmax = kNoallocMaxM
@@ -86,8 +87,17 @@ struct ScratchView {
 
 __global__ void noalloc_read_sumq_kernel(const GridDesc* g, float* out) { *out = g->sumQ_f; }
 
+// device memory of the current device: a pointer into another GPU's memory would be read by this device's
+// kernels through peer access, or fault without it
 void require_device(const void* p, const char* what) {
     require(is_device_ptr(p), std::string(what) + " must be device memory (this entry point stages nothing)");
+    cudaPointerAttributes a;
+    int dev = 0;
+    MGB_CUDA(cudaGetDevice(&dev));
+    MGB_CUDA(cudaPointerGetAttributes(&a, p));
+    require(a.type == cudaMemoryTypeManaged || a.device == dev,
+            std::string(what) + " is memory of device " + std::to_string(a.device) + ", not of the current device " +
+                std::to_string(dev));
 }
 
 }  // namespace
@@ -115,7 +125,10 @@ void fftconv_compute_noalloc(const float* K1h, const float* K2h, int M, int n_in
     cudaStream_t s = current_stream();
     ScratchView v(base, n_interp);
     GridDesc* g = reinterpret_cast<GridDesc*>(base + kGridOff);
-    // what must start at zero: the grid descriptor (last-block counter, flags) and the rows of W the spread uses
+    // what must start at zero: the grid descriptor (last-block counter, flags) and the rows of W the spread uses.
+    // The forward row pass clears every W row it reads, so after a completed call these rows are zero already;
+    // they are cleared here all the same, so that a call that stopped part-way (an error between two launches)
+    // leaves nothing behind for the next one, at the price of one pass over N x 512 float4 per call.
     const int N = n_boxes * n_interp;
     MGB_CUDA(cudaMemsetAsync(g, 0, sizeof(GridDesc), s));
     MGB_CUDA(cudaMemsetAsync(base + kWOff, 0, (size_t)N * kNoallocMaxM * sizeof(float4), s));

@@ -178,6 +178,44 @@ def optimize_tsne(P, Y, n_iter=750, early_iter=250, early_exaggeration=12.0, exa
     return Y
 
 
+def optimize_tsne_batch(Ps, Ys, n_iter=500, early_iter=None, early_exaggeration=12.0, exaggeration=1.0,
+                        learning_rate=None, momentum=(0.5, 0.8), n_interp=3, box_width=0.7, dof=1.0,
+                        max_boxes=None, threads_per_row=None, branches=None, autotune=True):
+    """Many independent t-SNE passes (each the device loop of optimize_tsne, magnet/tsne.py:132-214) run together:
+    one CUDA graph holds one iteration of every layout as independent branches, replayed n_iter times. Ps: the
+    layouts' symmetric CSR affinities (each normalised to sum 1 inside), Ys: their (n_i, 2) float32 initial layouts
+    (numpy or device arrays), updated in place and returned. early_iter None: min(250, n_iter // 3), MAGNET's
+    default for loss="tsne" (magnet/__init__.py:640). The learning rate, when None, is each layout's own
+    max(200, n_i / 12).
+
+    threads_per_row / branches None: the autotuner's cached choice for this batch's shape (magnet_b200.autotune),
+    tuned now when autotune is True and nothing is cached, else 8 lanes chosen from the row length and 32 branches.
+    max_boxes: per-layout grid allocation (None: 64 + 2 ceil(sqrt(n_i)))."""
+    from . import autotune as A
+    if early_iter is None:
+        early_iter = min(250, int(n_iter) // 3)
+    graphs = [_csr32(P) for P in Ps]
+    Ys = [Y if hasattr(Y, "__cuda_array_interface__") else np.ascontiguousarray(Y, dtype=np.float32) for Y in Ys]
+    params = dict(early_iter=int(early_iter), early_exaggeration=float(early_exaggeration),
+                  exaggeration=float(exaggeration), momentum_early=float(momentum[0]),
+                  momentum_late=float(momentum[1]), n_interp=int(n_interp), box_width=float(box_width),
+                  dof=float(dof), layout_max_boxes=None if max_boxes is None else [int(b) for b in max_boxes])
+    if learning_rate is not None:
+        params["learning_rate"] = float(learning_rate)
+    if threads_per_row is None or branches is None:
+        key = A.batch_key([g[0].size - 1 for g in graphs], [g[1].size for g in graphs])
+        choice = A.lookup(key)
+        if choice is None and autotune:
+            choice = A.tune_tsne_batch(graphs, Ys, params, key=key)
+        choice = choice or {"threads_per_row": 0, "branches": 32}
+        threads_per_row = choice["threads_per_row"] if threads_per_row is None else threads_per_row
+        branches = choice["branches"] if branches is None else branches
+    batch = N.TsneBatch(graphs, n_iter=int(n_iter), threads_per_row=int(threads_per_row), branches=int(branches),
+                        **params)
+    batch.run(Ys)
+    return Ys
+
+
 # ---------------------------------------------------------------------------------------------- SGD
 def sampling_frequencies(w, target):
     """freq_i = min(1, s w_i) with s solved exactly so that sum(freq) == target (magnet/__init__.py:51-66)."""

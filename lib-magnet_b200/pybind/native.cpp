@@ -280,6 +280,67 @@ py::tuple fuzzy_union(py::object ind, py::object vals, int64_t n, double set_op_
     return py::make_tuple(indptr, indices[py::slice(0, nnz, 1)], data[py::slice(0, nnz, 1)]);
 }
 
+// many t-SNE layouts run together (mg_tsne_batch_*): one CUDA graph per iteration holds every layout's kernels
+class TsneBatch {
+  public:
+    TsneBatch(py::list graphs, int n_iter, int early_iter, float early_exaggeration, float exaggeration,
+              float learning_rate, float momentum_early, float momentum_late, int n_interp, float box_width, float dof,
+              int min_boxes, int max_boxes, int threads_per_row, py::object layout_max_boxes, int branches) {
+        const size_t count = graphs.size();
+        std::vector<int64_t> n(count), nnz(count);
+        std::vector<const int32_t*> ip(count), ix(count);
+        std::vector<const float*> P(count);
+        std::vector<View<int32_t>> keep_i;
+        std::vector<View<float>> keep_f;
+        for (size_t i = 0; i < count; ++i) {
+            py::tuple t = graphs[i].cast<py::tuple>();
+            if (t.size() != 3) throw std::runtime_error("each layout is (indptr, indices, data)");
+            keep_i.push_back(view<int32_t>(t[0]));
+            keep_i.push_back(view<int32_t>(t[1]));
+            keep_f.push_back(view<float>(t[2]));
+            const auto& a = keep_i[keep_i.size() - 2];
+            const auto& b = keep_i.back();
+            n[i] = a.size() - 1; nnz[i] = b.size();
+            ip[i] = a.ptr; ix[i] = b.ptr; P[i] = keep_f.back().ptr;
+        }
+        std::vector<int> mb;
+        if (!layout_max_boxes.is_none()) mb = layout_max_boxes.cast<std::vector<int>>();
+        if (!mb.empty() && mb.size() != count) throw std::runtime_error("max_boxes needs one entry per layout");
+        mg_tsne_params p;
+        mg_tsne_params_default(&p);
+        p.n_iter = n_iter; p.early_iter = early_iter; p.early_exaggeration = early_exaggeration;
+        p.exaggeration = exaggeration; p.learning_rate = learning_rate; p.momentum_early = momentum_early;
+        p.momentum_late = momentum_late; p.n_interp = n_interp; p.box_width = box_width; p.dof = dof;
+        p.min_boxes = min_boxes; p.max_boxes = max_boxes; p.threads_per_row = threads_per_row;
+        py::gil_scoped_release rel;
+        check(mg_tsne_batch_create((int)count, n.data(), nnz.data(), ip.data(), ix.data(), P.data(), &p,
+                                   mb.empty() ? nullptr : mb.data(), branches, &h_));
+    }
+    ~TsneBatch() { mg_tsne_batch_destroy(h_); }
+    void run(py::list Ys) {
+        std::vector<View<float>> keep;
+        std::vector<float*> y;
+        for (size_t i = 0; i < Ys.size(); ++i) {
+            keep.push_back(view<float>(Ys[i]));
+            if (keep.back().ndim() != 2 || keep.back().dim(1) != 2) throw std::runtime_error("each Y must be (n, 2)");
+            y.push_back(keep.back().ptr);
+        }
+        int count = 0;
+        check(mg_tsne_batch_size(h_, &count, nullptr));
+        if ((int)y.size() != count) throw std::runtime_error("run needs one layout per graph of the batch");
+        py::gil_scoped_release rel;
+        check(mg_tsne_batch_run(h_, y.data()));
+    }
+    uint64_t kernels_per_iteration() const {
+        uint64_t k = 0;
+        check(mg_tsne_batch_size(h_, nullptr, &k));
+        return k;
+    }
+
+  private:
+    mg_tsne_batch* h_ = nullptr;
+};
+
 }  // namespace
 
 PYBIND11_MODULE(_native, m) {
@@ -429,6 +490,16 @@ PYBIND11_MODULE(_native, m) {
           py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("Y"), py::arg("n_iter"),
           py::arg("early_iter") = 0, py::arg("early_exaggeration") = 12.0f, py::arg("exaggeration") = 1.0f,
           py::arg("learning_rate") = -1.0f, py::arg("n_interp") = 3, py::arg("box_width") = 0.7f, py::arg("dof") = 1.0f);
+    py::class_<TsneBatch>(m, "TsneBatch", "many t-SNE layouts run together, one CUDA graph per iteration")
+        .def(py::init<py::list, int, int, float, float, float, float, float, int, float, float, int, int, int,
+                      py::object, int>(),
+             py::arg("graphs"), py::arg("n_iter") = 750, py::arg("early_iter") = 250,
+             py::arg("early_exaggeration") = 12.0f, py::arg("exaggeration") = 1.0f, py::arg("learning_rate") = -1.0f,
+             py::arg("momentum_early") = 0.5f, py::arg("momentum_late") = 0.8f, py::arg("n_interp") = 3,
+             py::arg("box_width") = 0.7f, py::arg("dof") = 1.0f, py::arg("min_boxes") = 20, py::arg("max_boxes") = 1000,
+             py::arg("threads_per_row") = 0, py::arg("layout_max_boxes") = py::none(), py::arg("branches") = 32)
+        .def("run", &TsneBatch::run, py::arg("Ys"))
+        .def_property_readonly("kernels_per_iteration", &TsneBatch::kernels_per_iteration);
     m.def("center_scale", [](py::object Y, double target_std) {
               auto y = view<float>(Y);
               if (y.ndim() != 2) throw std::runtime_error("Y must be (n, dim)");

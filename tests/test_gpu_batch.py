@@ -1,0 +1,83 @@
+"""The batched form: many t-SNE layouts of uneven size run together (one CUDA graph per iteration, the layouts as
+independent branches). Each layout must come out as the single-layout device loop makes it, and as the
+reference's own optimize_tsne (magnet/tsne.py:132-214, its compiled kernels on the host) makes it: KL within 1 %
+and 15-NN preservation within 0.01 per layout. The autotuner's choice is cached by the batch's shape."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+import quality  # noqa: E402
+import bench  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def instance(n, seed, d=32):
+    """a perplexity-30 layout problem: a Gaussian mixture of 3-8 components in d = 32, its 90-NN affinities and a
+    PCA start scaled to std 1e-4, as the batched configuration builds its instances"""
+    rng = np.random.default_rng(seed)
+    k = int(rng.integers(3, 9))
+    C = rng.normal(0, 5, (k, d))
+    X = (C[rng.integers(0, k, n)] + rng.normal(0, 1, (n, d))).astype(np.float32)
+    ind, d2 = bench.exact_knn_cpu(X, min(90, n - 1))
+    P = bench.perplexity_affinities(ind, d2, 30.0)
+    Y0 = bench.pca_init(X, seed)
+    return X, P, np.ascontiguousarray(Y0 / max(float(Y0[:, 0].std()), 1e-12) * 1e-4, dtype=np.float32)
+
+
+@pytest.fixture(scope="module")
+def problems():
+    return [instance(n, 100 + i) for i, n in enumerate([500, 900, 1500, 2600, 4100, 6500])]
+
+
+def test_batch_matches_single_layout_loop(mg, problems):
+    Ys = [Y0.copy() for _, _, Y0 in problems]
+    mg.optimize_tsne_batch([P for _, P, _ in problems], Ys, n_iter=150, threads_per_row=8, branches=4)
+    for (X, P, Y0), Yb in zip(problems, Ys):
+        Ys1 = mg.optimize_tsne(P, Y0.copy(), n_iter=150, early_iter=50, threads_per_row=8)
+        assert np.isfinite(Yb).all()
+        kb, k1 = quality.kl_divergence(P, Yb), quality.kl_divergence(P, Ys1)
+        nb, n1 = quality.knn_preservation(X, Yb), quality.knn_preservation(X, Ys1)
+        print("n=%d KL batch %.4f single %.4f; 15-NN batch %.4f single %.4f" % (len(X), kb, k1, nb, n1))
+        assert abs(kb - k1) / k1 < 0.005 and abs(nb - n1) < 0.01
+
+
+def test_batch_against_reference_loop(mg, ref, problems):
+    if ref is None:
+        pytest.skip("reference module not built")
+    sub = problems[:4]
+    Ys = [Y0.copy() for _, _, Y0 in sub]
+    mg.optimize_tsne_batch([P for _, P, _ in sub], Ys, n_iter=200, branches=3, threads_per_row=4)
+    for (X, P, Y0), Yb in zip(sub, Ys):
+        Yr = O.optimize_tsne(P, Y0.copy(), n_iter=200, early_iter=66, n_threads=-1, backend="reference")
+        kb, kr = quality.kl_divergence(P, Yb), quality.kl_divergence(P, Yr)
+        nb, nr = quality.knn_preservation(X, Yb), quality.knn_preservation(X, Yr)
+        print("n=%d KL batch %.4f reference %.4f; 15-NN batch %.4f reference %.4f" % (len(X), kb, kr, nb, nr))
+        assert abs(kb - kr) / kr < 0.01 and abs(nb - nr) < 0.01
+
+
+def test_autotuner_caches_its_choice(mg, problems, tmp_path, monkeypatch):
+    from magnet_b200 import autotune as A
+    monkeypatch.setenv("MAGNET_B200_CACHE", str(tmp_path))
+    sub = problems[:3]
+    Ys = [Y0.copy() for _, _, Y0 in sub]
+    mg.optimize_tsne_batch([P for _, P, _ in sub], Ys, n_iter=30)
+    key = A.batch_key([len(X) for X, _, _ in sub], [P.nnz for _, P, _ in sub])
+    choice = A.lookup(key)
+    assert choice is not None and choice["threads_per_row"] in A.TPR and choice["branches"] in A.BRANCHES
+    assert os.path.exists(A.cache_path())
+    assert all(np.isfinite(Y).all() for Y in Ys)
+
+
+def test_batch_rejects_bad_arguments(mg, problems):
+    _, P, Y0 = problems[0]
+    g = [(P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data.astype(np.float32))]
+    with pytest.raises(RuntimeError, match="branches"):
+        mg._native.TsneBatch(g, n_iter=5, branches=0)
+    b = mg._native.TsneBatch(g, n_iter=5, branches=2)
+    with pytest.raises(RuntimeError, match="one layout per graph"):
+        b.run([Y0.copy(), Y0.copy()])
