@@ -915,6 +915,18 @@ def serve_stream(draw, n_requests, rate, fit_sizes, seed):
     return sizes, gaps, batches, fit_at
 
 
+def transform_knn15(X_train, Y_train, X_new, Y_new, k=15, limit=3000):
+    """15-NN preservation of transformed rows: each new row's k nearest training rows in the data against the k
+    nearest training rows of its layout position (the first `limit` new rows), mean overlap / k"""
+    from sklearn.neighbors import NearestNeighbors
+    from scipy.spatial import cKDTree
+    Xn, Yn = np.asarray(X_new[:limit]), np.asarray(Y_new[:limit], dtype=np.float64)
+    hi = NearestNeighbors(n_neighbors=k, algorithm="brute", n_jobs=-1).fit(X_train).kneighbors(
+        Xn, return_distance=False)
+    lo = cKDTree(np.asarray(Y_train, dtype=np.float64)).query(Yn, k, workers=-1)[1]
+    return float(np.mean([len(np.intersect1d(a, b)) / k for a, b in zip(hi, lo)]))
+
+
 def reference_serve(n_requests=300, rate=200.0, fit_sizes=(5000, 20000, 50000), seed=3, n_train=200_000):
     """The served workload on the reference's CPU path (its compiled module on all host threads, driven as
     MAGNET.fit / MAGNET.transform drive it): the same fitted 200k x 64 layout, built by the reference, and the
@@ -934,10 +946,11 @@ def reference_serve(n_requests=300, rate=200.0, fit_sizes=(5000, 20000, 50000), 
     arrivals = np.cumsum(gaps)
     clock = 0.0
     lat_t, lat_f = [], []
+    placed = []
     for i in range(n_requests):
         start = max(arrivals[i], clock)
         t = time.perf_counter()
-        O.reference_transform(X, P, Y, landmarks, step, batches[i], a=a, b=b, n_epochs=100, seed=i)
+        placed.append(O.reference_transform(X, P, Y, landmarks, step, batches[i], a=a, b=b, n_epochs=100, seed=i))
         clock = start + (time.perf_counter() - t)
         lat_t.append(clock - arrivals[i])
         if i in fit_at:
@@ -953,7 +966,8 @@ def reference_serve(n_requests=300, rate=200.0, fit_sizes=(5000, 20000, 50000), 
         return {"requests": len(lat), "p50_ms": round(float(np.percentile(lat, 50)), 2),
                 "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
                 "points_per_s": round(pts / max(span, 1e-9), 2)}
-    return {"transform": summary(lat_t, int(sizes.sum())) | {"slots": 1},
+    knn15 = transform_knn15(X, Y, np.concatenate(batches), np.concatenate(placed))
+    return {"transform": summary(lat_t, int(sizes.sum())) | {"slots": 1, "knn15": round(knn15, 4)},
             "fit_requests": summary(lat_f, int(sum(len(v) for v in fit_at.values()))),
             "serve_config": {"layout": "200,000 x 64, 50-Gaussian mixture, seed 3, k=15 (built by the reference)",
                              "requests": n_requests, "rate_per_s": rate, "batch": "uniform integer [1, 4096]",
@@ -970,9 +984,9 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
     import magnet_b200 as mg
     t0 = time.perf_counter()
     X, draw = serve_workload(seed=seed)
-    Y = S.fit_layout(X, n_epochs=200, seed=0)
+    Y, P = S.fit_layout(X, n_epochs=200, seed=0, return_graph=True)
     a, b = mg.find_ab_params(1.0, 0.1)
-    layout = S.FittedLayout(X, Y, a=a, b=b, transform_epochs=100)
+    layout = S.FittedLayout(X, Y, a=a, b=b, transform_epochs=100, graph=P)
     setup_s = time.perf_counter() - t0
     sizes, gaps, batches, fit_at = serve_stream(draw, n_requests, rate, fit_sizes, seed)
     big = batches[int(np.argmax(sizes))]
@@ -984,7 +998,7 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
         for f in warm:
             f.result()
         srv.done.clear()
-        futs = []
+        futs, kinds = [], []
         t_next = time.perf_counter()
         for i in range(n_requests):
             t_next += gaps[i]
@@ -993,15 +1007,19 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
                 time.sleep(dt)
             m = int(sizes[i])
             futs.append(srv.submit("transform", (batches[i], i), layout.request_bytes(m), m))
+            kinds.append("transform")
             if i in fit_at:
                 Xf = fit_at[i]
                 futs.append(srv.submit("fit", Xf, S.fit_bytes(len(Xf), X.shape[1]), len(Xf)))
-        for f in futs:
-            f.result()
+                kinds.append("fit")
+        res = [f.result() for f in futs]
         srv.close()
+        placed = [r for r, kind in zip(res, kinds) if kind == "transform"]
         tr = S.latency_summary(srv.done, "transform")
         fi = S.latency_summary(srv.done, "fit")
-        return {k2: round(v, 2) for k2, v in tr.items()}, {k2: round(v, 1) for k2, v in fi.items()}
+        tr["knn15"] = transform_knn15(X, Y, np.concatenate(batches), np.concatenate(placed))
+        return {k2: round(v, 4 if k2 == "knn15" else 2) for k2, v in tr.items()}, \
+            {k2: round(v, 1) for k2, v in fi.items()}
 
     plain, plain_fit = run(1)
     mixed, mixed_fit = run(slots)
@@ -1010,6 +1028,7 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
             "serve_config": {"layout": "200,000 x 64, 50-Gaussian mixture, seed 3, k=15, resident",
                              "requests": n_requests, "rate_per_s": rate, "batch": "uniform integer [1, 4096]",
                              "transform_epochs": 100, "fits": list(fit_sizes), "mode": "owner",
+                             "query_knn": "beam search over the training graph (device)",
                              "setup_s": round(setup_s, 1)}}
 
 

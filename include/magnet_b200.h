@@ -208,7 +208,7 @@ int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* sampled, int
  * log2(n_neighbors) * bandwidth in n_iter steps at most. */
 int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter, float* out);
 
-/* mid_near_pairs_dense (src/nndescent.cpp:731-768, bound at src/bindings.cpp:66-67): X (n, d) dense rows -> out
+/* mid_near_pairs_dense (src/nndescent.cpp:731-768, bound at src/bindings.cpp:58-59): X (n, d) dense rows -> out
  * (n, n_pairs), for every row and pair the second closest, by squared distance then index, of n_cand rows drawn
  * at random (the row itself replaced by the next row). The draws are the reference's streams for n_threads threads
  * (<= 0: the host's hardware threads, as the reference resolves it; the partners depend on it as the reference's
@@ -217,6 +217,17 @@ int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float ba
  * (MG_ERR_ARGUMENT otherwise, with the reference's message). Synchronous. */
 int mg_mid_near_pairs(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed, int n_threads,
                       int32_t* out);
+
+/* knn_search (src/nndescent.cpp:585-690, bound at src/bindings.cpp:43-45; called by MAGNET.transform through
+ * magnet/knn.py:131-152): the k nearest training rows of each query row by beam search over the training rows'
+ * neighbour graph (gptr n + 1, gidx nnz), started from the n_entry landmarks closest to the query (n_land > 0) or
+ * from n_entry random rows drawn as the reference draws them for n_threads threads. X (n, d) training rows, Q (m, d)
+ * queries; out_i / out_d (m, k) rows and squared distances sorted by (distance, row), -1 / inf past the rows found.
+ * Distances follow the reference's kernel for the host's instruction set, so the results equal the reference's
+ * wherever no two distances tie. 1 <= k <= n, k <= ef <= 256. Synchronous. */
+int mg_knn_search(const float* X, int64_t n, int d, const int32_t* gptr, const int32_t* gidx, int64_t nnz,
+                  const int32_t* landmarks, int64_t n_land, const float* Q, int64_t m, int k, int ef, int n_entry,
+                  uint64_t seed, int n_threads, int32_t* out_i, float* out_d);
 
 /* The fuzzy union of fuzzy_graph (magnet/knn.py:215-230, after smooth_knn): A = the n x n matrix with rows
  * i < n_rows holding (ind[i, j], vals[i, j]) (duplicate columns summed, zeros dropped), and

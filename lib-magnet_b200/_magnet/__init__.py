@@ -2,8 +2,8 @@
 
 Put the directory holding this package ahead of the reference's extension on sys.path; the reference's Python
 package (`magnet`) then runs its layout pass on the B200: optimize_layout, FFTConv2D, tsne_attraction, tsne_step,
-tsne_update, bbox_2d, mid_spring, smooth_knn and mid_near_pairs_dense come from the device library. The host-side
-kernels that stay on the reference's code (nn_descent, knn_search, sparse mid-near pairs, spectral init, louvain)
+tsne_update, bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense and knn_search come from the device library. The
+host-side kernels that stay on the reference's code (nn_descent, the sparse-data searches, spectral init, louvain)
 are forwarded to the reference's own compiled module, found through the MAGNET_HOST_MODULE environment variable
 (path to the reference's `_magnet*.so`); without it they raise ImportError when used, as a missing `_magnet` would.
 """
@@ -12,9 +12,9 @@ import os as _os
 import sys as _sys
 
 from magnet_b200._native import (FFTConv2D, optimize_layout, tsne_attraction, tsne_step, tsne_update,  # noqa: F401
-                                 bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense)
+                                 bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense, knn_search)
 
-_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search", "knn_search_sparse", "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration", "louvain", "interp_scatter",
+_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search_sparse", "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration", "louvain", "interp_scatter",
                "interp_gather", "scatter_padded_2d", "spectral_products", "gather_forces_2d", "umap_attraction")
 
 

@@ -699,6 +699,54 @@ extern "C" int mg_mid_near_pairs(const float* X, int64_t n, int d, int n_pairs, 
     });
 }
 
+extern "C" int mg_knn_search(const float* X, int64_t n, int d, const int32_t* gptr, const int32_t* gidx, int64_t nnz,
+                             const int32_t* landmarks, int64_t n_land, const float* Q, int64_t m, int k, int ef,
+                             int n_entry, uint64_t seed, int n_threads, int32_t* out_i, float* out_d) {
+    return guard([&] {
+        // src/nndescent.cpp:666-674
+        require(X && d >= 1 && n >= 1 && m >= 0 && (m == 0 || Q), "X and Q must be 2-d with the same width");
+        require(k >= 1 && k <= n && ef >= k, "need 1 <= k <= n and ef >= k");
+        require(ef <= knn_search_max_ef(), "ef above " + std::to_string(knn_search_max_ef()) + " is not supported");
+        require(n_entry >= 1, "n_entry must be positive");
+        require(n <= INT32_MAX, "n must fit 32-bit indices");
+        require(gptr && (nnz == 0 || gidx) && (m == 0 || (out_i && out_d)), "arrays must not be NULL");
+        require(n_land == 0 || landmarks, "landmarks must not be NULL");
+        validate_csr_host(gptr, gidx, nnz, n, -1, "knn_search");
+        if (landmarks && !is_device_ptr(landmarks))
+            for (int64_t l = 0; l < n_land; ++l)
+                require(landmarks[l] >= 0 && landmarks[l] < n, "landmark out of range");
+        std::vector<int32_t> entries;
+        if (n_land == 0 && m > 0) {
+            // the reference's random entry rows: thread t of nt draws for queries t, t + nt, ... from
+            // Rng(seed + 7 (t + 1)) (src/nndescent.cpp:677-685)
+            if (n_threads <= 0) {
+                const unsigned h = std::thread::hardware_concurrency();
+                n_threads = h == 0 ? 4 : (int)h;
+            }
+            const int64_t nt = std::min<int64_t>(n_threads, std::max<int64_t>(1, m / 64));
+            entries.resize((size_t)m * n_entry);
+            for (int64_t t = 0; t < nt; ++t) {
+                Rng rng(seed + 7ULL * (uint64_t)(t + 1));
+                for (int64_t q = t; q < m; q += nt)
+                    for (int e = 0; e < n_entry; ++e) entries[(size_t)q * n_entry + e] = (int32_t)rng.below((uint32_t)n);
+            }
+        }
+        cudaStream_t s = current_stream();
+        const float* Xd = in_dev(X, n * (int64_t)d, 0, s);
+        const int32_t* gp = in_dev(gptr, n + 1, 1, s);
+        const int32_t* gx = in_dev(gidx, nnz, 2, s);
+        const int32_t* ld = in_dev(landmarks, n_land, 3, s);
+        const float* Qd = in_dev(Q, m * (int64_t)d, 4, s);
+        int32_t* oi = out_dev(out_i, m * (int64_t)k, 5);
+        float* od = out_dev(out_d, m * (int64_t)k, 6);
+        knn_search_dev(Xd, n, d, gp, gx, ld, n_land, entries.data(), Qd, m, k, ef, n_entry, host_distance_order(), oi,
+                       od, s);
+        back(out_i, oi, m * (int64_t)k, s);
+        back(out_d, od, m * (int64_t)k, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 extern "C" int mg_fuzzy_union(const int32_t* ind, const float* vals, int64_t n_rows, int k, int64_t n,
                               double set_op_mix_ratio, int32_t* indptr, int32_t* indices, float* data, int64_t cap,
                               int64_t* nnz) {

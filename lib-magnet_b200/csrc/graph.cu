@@ -351,6 +351,10 @@ __global__ void narrow_kernel(const int64_t* __restrict__ in, int64_t n, int32_t
 
 }  // namespace
 
+void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, DevBuf& tmp, cudaStream_t s) {
+    exclusive_scan(in, n, out, tmp, s);
+}
+
 void smooth_knn_dev(const float* dist, int64_t n_rows, int k, float target, int n_iter, float* out, GraphWork& w,
                     cudaStream_t s) {
     if (n_rows == 0 || k == 0) return;

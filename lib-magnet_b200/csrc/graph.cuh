@@ -27,6 +27,16 @@ int64_t fuzzy_union_dev(const int32_t* ind, const float* vals, int64_t n_rows, i
 // threads (>= 1) and its squared-distance kernel `order` (0 AVX-512, 1 AVX2, 2 plain loop).
 void mid_near_pairs_dev(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed, int n_threads,
                         int order, int32_t* out, GraphWork& w, cudaStream_t s);
+// out[0..n] = exclusive scan of in[0..n) and, in out[n], the total (tmp: tile sums)
+void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, DevBuf& tmp, cudaStream_t s);
+// knn_search (src/nndescent.cpp:585-690): the beam search of queries Q (m, d) over the training rows X (n, d) and
+// their neighbour graph (gptr, gidx), from the n_entry landmarks closest to each query, or from the given random
+// entry rows (host array m x n_entry) without landmarks; out (m, k) rows and squared distances. ef <=
+// knn_search_max_ef(). Synchronises s.
+void knn_search_dev(const float* X, int64_t n, int d, const int32_t* gptr, const int32_t* gidx, const int32_t* land,
+                    int64_t n_land, const int32_t* entries_host, const float* Q, int64_t m, int k, int ef,
+                    int n_entry, int order, int32_t* out_i, float* out_d, cudaStream_t s);
+int knn_search_max_ef();
 // the reference's distance kernel on this host (its CPUID choice, src/nndescent.cpp:101-106)
 int host_distance_order();
 

@@ -16,6 +16,7 @@
 // tail fused), AVX2 (8 lanes, ((0+1)+(2+3))+((4+5)+(6+7)), the tail fused) or the plain loop (4 interleaved sums,
 // no fusion), each written with explicit rounding intrinsics so the compiler neither fuses nor reorders them.
 #include "graph.cuh"
+#include "sqdist.cuh"
 #include <vector>
 #include <thread>
 #include <algorithm>
@@ -97,46 +98,6 @@ __global__ void __launch_bounds__(256) mid_state_kernel(const uint64_t* __restri
     for (int64_t r = first; r < last; ++r) {
         row_state[r] = s;
         for (int t = 0; t < draws_per_row; ++t) s = xs_step(s);
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ float sqdist(const float* __restrict__ a, const float* __restrict__ b, int d) {
-    if constexpr (ORDER == 2) {
-        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-        int i = 0;
-        for (; i + 4 <= d; i += 4) {
-            const float d0 = __fsub_rn(a[i], b[i]), d1 = __fsub_rn(a[i + 1], b[i + 1]);
-            const float d2 = __fsub_rn(a[i + 2], b[i + 2]), d3 = __fsub_rn(a[i + 3], b[i + 3]);
-            s0 = __fadd_rn(s0, __fmul_rn(d0, d0)); s1 = __fadd_rn(s1, __fmul_rn(d1, d1));
-            s2 = __fadd_rn(s2, __fmul_rn(d2, d2)); s3 = __fadd_rn(s3, __fmul_rn(d3, d3));
-        }
-        for (; i < d; ++i) { const float df = __fsub_rn(a[i], b[i]); s0 = __fadd_rn(s0, __fmul_rn(df, df)); }
-        return __fadd_rn(__fadd_rn(s0, s1), __fadd_rn(s2, s3));
-    } else {
-        constexpr int L = ORDER == 0 ? 16 : 8;
-        float acc[L];
-#pragma unroll
-        for (int l = 0; l < L; ++l) acc[l] = 0.f;
-        int i = 0;
-        for (; i + L <= d; i += L) {
-#pragma unroll
-            for (int l = 0; l < L; ++l) { const float df = __fsub_rn(a[i + l], b[i + l]); acc[l] = __fmaf_rn(df, df, acc[l]); }
-        }
-        float s;
-        if constexpr (ORDER == 0) {
-            float t3[8], t6[4];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) t3[k] = __fadd_rn(acc[8 + k], acc[k]);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) t6[k] = __fadd_rn(t3[4 + k], t3[k]);
-            s = __fadd_rn(__fadd_rn(t6[0], t6[2]), __fadd_rn(t6[1], t6[3]));
-        } else {
-            s = __fadd_rn(__fadd_rn(__fadd_rn(acc[0], acc[1]), __fadd_rn(acc[2], acc[3])),
-                          __fadd_rn(__fadd_rn(acc[4], acc[5]), __fadd_rn(acc[6], acc[7])));
-        }
-        for (; i < d; ++i) { const float df = __fsub_rn(a[i], b[i]); s = __fmaf_rn(df, df, s); }
-        return s;
     }
 }
 

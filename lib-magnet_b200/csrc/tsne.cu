@@ -9,8 +9,10 @@
 //    captured CUDA graph is replayed for all iterations.
 #include "tsne.cuh"
 #include "interp.cuh"
+#include "graph.cuh"
 #include <vector>
 #include <algorithm>
+#include <cstdlib>
 
 namespace mgb {
 
@@ -414,6 +416,103 @@ __global__ void init_opt_state_kernel(float2* U, float2* G, int64_t n) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------- spatial order
+constexpr int kOrderBits = 10;                     // box index bits per axis (n_boxes <= 1000 < 2^10)
+constexpr int64_t kOrderBins = 1LL << (2 * kOrderBits);
+constexpr int64_t kReorderMinPoints = 20000;       // smaller layouts stay in L1 / L2 whatever their order
+
+__device__ __forceinline__ uint32_t morton_spread(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// the Morton index of each point's box in the last iteration's grid (positions with the pending recentring)
+__global__ void order_key_kernel(const float2* __restrict__ Y, int64_t n, const GridDesc* __restrict__ g,
+                                 int32_t* __restrict__ key, int32_t* __restrict__ cnt) {
+    const bool rc = g->recentre != 0;
+    const float mx = g->mean[0], my = g->mean[1];
+    const float xmin = g->xmin, ymin = g->ymin, inv_w = g->inv_width;
+    const float top = (float)max(g->n_boxes - 1, 0);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float2 p = Y[i];
+        if (rc) { p.x -= mx; p.y -= my; }
+        const float fx = fminf(fmaxf((p.x - xmin) * inv_w, 0.f), top);   // NaN -> 0
+        const float fy = fminf(fmaxf((p.y - ymin) * inv_w, 0.f), top);
+        const int32_t k = (int32_t)(morton_spread((uint32_t)fx) | (morton_spread((uint32_t)fy) << 1));
+        key[i] = k;
+        atomicAdd(&cnt[k], 1);
+    }
+}
+
+// counting-sort scatter: the new row of point i (cursor = the bin counts, cleared)
+__global__ void order_scatter_kernel(const int32_t* __restrict__ key, int64_t n, const int64_t* __restrict__ start,
+                                     int32_t* __restrict__ cursor, int32_t* __restrict__ src,
+                                     int32_t* __restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = key[i];
+        const int64_t r = start[k] + atomicAdd(&cursor[k], 1);
+        src[r] = (int32_t)i;
+        dst[i] = (int32_t)r;
+    }
+}
+
+// per-point state into the new order; the new rows' affinity row lengths
+__global__ void order_gather_kernel(const int32_t* __restrict__ src, int64_t n, const float2* __restrict__ Y,
+                                    const float2* __restrict__ U, const float2* __restrict__ G,
+                                    const int32_t* __restrict__ perm, bool permuted, const int32_t* __restrict__ ip,
+                                    float2* __restrict__ Yt, float2* __restrict__ Ut, float2* __restrict__ Gt,
+                                    int32_t* __restrict__ perm_t, int32_t* __restrict__ len) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t o = src[r];
+        Yt[r] = Y[o]; Ut[r] = U[o]; Gt[r] = G[o];
+        perm_t[r] = permuted ? perm[o] : o;
+        len[r] = ip[o + 1] - ip[o];
+    }
+}
+
+// one warp per new row: the old row's entries, column indices relabelled
+__global__ void order_csr_kernel(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t n,
+                                 const int32_t* __restrict__ ip, const int32_t* __restrict__ ix,
+                                 const float* __restrict__ P, const int64_t* __restrict__ newptr,
+                                 int32_t* __restrict__ ipt, int32_t* __restrict__ ixt, float* __restrict__ Pt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+        const int32_t o = src[r];
+        const int32_t b = ip[o], e = ip[o + 1];
+        const int64_t out = newptr[r];
+        for (int32_t j = b + lane; j < e; j += 32) {
+            ixt[out + (j - b)] = dst[ix[j]];
+            Pt[out + (j - b)] = P[j];
+        }
+        if (lane == 0) ipt[r] = (int32_t)out;
+        if (r == n - 1 && lane == 0) ipt[n] = (int32_t)newptr[n];
+    }
+}
+
+// the caller's layout into the current row order (Ynext[r] = Y[perm[r]])
+__global__ void order_in_kernel(const float2* __restrict__ Yin, const int32_t* __restrict__ perm, int64_t n,
+                                float2* __restrict__ Y) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        Y[r] = Yin[perm[r]];
+}
+
+// the recentred layout back into the caller's order (Yout[perm[r]] = Ynext[r] - mean)
+__global__ void finish_layout_perm_kernel(const float2* __restrict__ Ynext, const int32_t* __restrict__ perm,
+                                          float2* __restrict__ Yout, int64_t n, const GridDesc* __restrict__ g) {
+    const bool rc = g->recentre != 0;
+    const float mx = g->mean[0], my = g->mean[1];
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        float2 p = Ynext[r];
+        if (rc) { p.x = __fsub_rn(p.x, mx); p.y = __fsub_rn(p.y, my); }
+        Yout[perm[r]] = p;
+    }
+}
+
 template <int NI, int T>
 void launch_iter_t(TsneDev& d, cudaStream_t st) {
     loop_iter_kernel<NI, T><<<d.blocks_iter, kThreads, 0, st>>>(
@@ -537,6 +636,10 @@ void TsneDev::init(const int32_t* ip_h, const int32_t* ix_h, const float* P_h, i
     require(s.ni >= 1 && s.ni <= 8, "n_interp must be between 1 and 8");
     require(s.min_boxes >= 1 && s.max_boxes >= s.min_boxes, "invalid box limits");
     n = n_; nnz = nnz_; ni = s.ni; sch = s; dof = dof_;
+    permuted = false;   // the affinities are copied afresh below, in the caller's order
+    // MAGNET_TSNE_REORDER_EVERY: iterations between spatial reorders (0 turns them off)
+    if (const char* v = std::getenv("MAGNET_TSNE_REORDER_EVERY")) reorder_every = std::max(0, std::atoi(v));
+    else reorder_every = 25;
     if (threads_per_row <= 0) {
         const double deg = n > 0 ? (double)nnz / (double)n : 0.0;
         tpr = deg < 3 ? 1 : deg < 6 ? 2 : deg < 12 ? 4 : deg < 40 ? 8 : deg < 100 ? 16 : 32;
@@ -588,7 +691,18 @@ std::string TsneDev::signature() const {
 }
 
 void TsneDev::set_layout(const float* Y, bool host, cudaStream_t st) {
-    MGB_CUDA(cudaMemcpyAsync(Ynext.p, Y, sizeof(float2) * n, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+    if (permuted) {
+        // rows are in the spatial order of the previous run: bring the caller's layout into it
+        Yt.ensure(sizeof(float2) * n);
+        MGB_CUDA(cudaMemcpyAsync(Yt.p, Y, sizeof(float2) * n, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                 st));
+        order_in_kernel<<<grid_blocks(n, kThreads), kThreads, 0, st>>>(Yt.as<float2>(), perm.as<int32_t>(), n,
+                                                                          Ynext.as<float2>());
+        MGB_LAUNCH_CHECK();
+    } else {
+        MGB_CUDA(cudaMemcpyAsync(Ynext.p, Y, sizeof(float2) * n, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                 st));
+    }
     init_opt_state_kernel<<<grid_blocks(n, kThreads), kThreads, 0, st>>>(U.as<float2>(), G.as<float2>(), n);
     MGB_LAUNCH_CHECK();
     // no pending recentring, iteration 0, empty spectrum and twiddle keys
@@ -599,6 +713,17 @@ void TsneDev::set_layout(const float* Y, bool host, cudaStream_t st) {
 }
 
 void TsneDev::get_layout(float* Y, bool host, cudaStream_t st) {
+    if (permuted) {
+        float2* out = host ? Ycur.as<float2>() : reinterpret_cast<float2*>(Y);
+        finish_layout_perm_kernel<<<grid_blocks(n, kThreads), kThreads, 0, st>>>(Ynext.as<float2>(), perm.as<int32_t>(),
+                                                                                 out, n, g());
+        MGB_LAUNCH_CHECK();
+        if (host) {
+            MGB_CUDA(cudaMemcpyAsync(Y, Ycur.p, sizeof(float2) * n, cudaMemcpyDeviceToHost, st));
+            MGB_CUDA(cudaStreamSynchronize(st));
+        }
+        return;
+    }
     if (host) {
         finish_layout_kernel<<<grid_blocks(n, kThreads), kThreads, 0, st>>>(Ynext.as<float2>(), Ycur.as<float2>(), n, g());
         MGB_LAUNCH_CHECK();
@@ -638,10 +763,59 @@ void TsneDev::iterate(cudaStream_t st, cudaEvent_t* ev) {
     mark(8);
 }
 
+bool TsneDev::reorder_due(int i) const {
+    return reorder_every > 0 && n >= kReorderMinPoints && n <= INT32_MAX && i % reorder_every == 1;
+}
+
+void TsneDev::reorder(cudaStream_t st) {
+    const int blocks = grid_blocks(n, kThreads);
+    okey.ensure(sizeof(int32_t) * n);
+    ocnt.ensure(sizeof(int32_t) * kOrderBins);
+    ostart.ensure(sizeof(int64_t) * (kOrderBins + 1));
+    osrc.ensure(sizeof(int32_t) * n); onew.ensure(sizeof(int32_t) * n); olen.ensure(sizeof(int32_t) * n);
+    oip.ensure(sizeof(int64_t) * (n + 1));
+    Yt.ensure(sizeof(float2) * n); Ut.ensure(sizeof(float2) * n); Gt.ensure(sizeof(float2) * n);
+    perm.ensure(sizeof(int32_t) * n); perm_t.ensure(sizeof(int32_t) * n);
+    ipt.ensure(sizeof(int32_t) * (n + 1));
+    ixt.ensure(sizeof(int32_t) * std::max<int64_t>(nnz, 1)); Pt.ensure(sizeof(float) * std::max<int64_t>(nnz, 1));
+    MGB_CUDA(cudaMemsetAsync(ocnt.p, 0, sizeof(int32_t) * kOrderBins, st));
+    order_key_kernel<<<blocks, kThreads, 0, st>>>(Ynext.as<float2>(), n, g(), okey.as<int32_t>(), ocnt.as<int32_t>());
+    MGB_LAUNCH_CHECK();
+    exclusive_scan_i32(ocnt.as<int32_t>(), kOrderBins, ostart.as<int64_t>(), oscan, st);
+    MGB_CUDA(cudaMemsetAsync(ocnt.p, 0, sizeof(int32_t) * kOrderBins, st));
+    order_scatter_kernel<<<blocks, kThreads, 0, st>>>(okey.as<int32_t>(), n, ostart.as<int64_t>(), ocnt.as<int32_t>(),
+                                                      osrc.as<int32_t>(), onew.as<int32_t>());
+    MGB_LAUNCH_CHECK();
+    order_gather_kernel<<<blocks, kThreads, 0, st>>>(osrc.as<int32_t>(), n, Ynext.as<float2>(), U.as<float2>(),
+                                                     G.as<float2>(), perm.as<int32_t>(), permuted, ip.as<int32_t>(),
+                                                     Yt.as<float2>(), Ut.as<float2>(), Gt.as<float2>(),
+                                                     perm_t.as<int32_t>(), olen.as<int32_t>());
+    MGB_LAUNCH_CHECK();
+    exclusive_scan_i32(olen.as<int32_t>(), n, oip.as<int64_t>(), oscan, st);
+    order_csr_kernel<<<grid_blocks(n * 32, kThreads), kThreads, 0, st>>>(
+        osrc.as<int32_t>(), onew.as<int32_t>(), n, ip.as<int32_t>(), ix.as<int32_t>(), P.as<float>(), oip.as<int64_t>(),
+        ipt.as<int32_t>(), ixt.as<int32_t>(), Pt.as<float>());
+    MGB_LAUNCH_CHECK();
+    // back into the buffers the captured iteration reads
+    MGB_CUDA(cudaMemcpyAsync(Ynext.p, Yt.p, sizeof(float2) * n, cudaMemcpyDeviceToDevice, st));
+    MGB_CUDA(cudaMemcpyAsync(U.p, Ut.p, sizeof(float2) * n, cudaMemcpyDeviceToDevice, st));
+    MGB_CUDA(cudaMemcpyAsync(G.p, Gt.p, sizeof(float2) * n, cudaMemcpyDeviceToDevice, st));
+    MGB_CUDA(cudaMemcpyAsync(perm.p, perm_t.p, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+    MGB_CUDA(cudaMemcpyAsync(ip.p, ipt.p, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToDevice, st));
+    if (nnz > 0) {
+        MGB_CUDA(cudaMemcpyAsync(ix.p, ixt.p, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, st));
+        MGB_CUDA(cudaMemcpyAsync(P.p, Pt.p, sizeof(float) * nnz, cudaMemcpyDeviceToDevice, st));
+    }
+    permuted = true;
+}
+
 void TsneDev::run(int n_iter, bool use_graph, cudaStream_t st) {
     if (n_iter <= 0) return;
     if (!use_graph) {
-        for (int i = 0; i < n_iter; ++i) iterate(st);
+        for (int i = 0; i < n_iter; ++i) {
+            if (reorder_due(i)) reorder(st);
+            iterate(st);
+        }
         return;
     }
     if (graph && graph_stream != st) { cudaGraphExecDestroy(graph); graph = nullptr; }
@@ -671,6 +845,7 @@ void TsneDev::run(int n_iter, bool use_graph, cudaStream_t st) {
         count_launch(0 - graph_kernels);   // captured, not run: the replays below count them
     }
     for (int i = 0; i < n_iter; ++i) {
+        if (reorder_due(i)) reorder(st);
         MGB_CUDA(cudaGraphLaunch(graph, st));
         count_launch(graph_kernels);
     }
@@ -681,6 +856,16 @@ void TsneDev::run_profiled(int n_iter, cudaStream_t st, double* stage_ms, int* g
     for (auto& e : ev) MGB_CUDA(cudaEventCreate(&e));
     try {
         for (int it = 0; it < n_iter; ++it) {
+            float ro = 0.f;
+            if (reorder_due(it)) {   // counted with stage 0 (bbox + grid choice) and in the total
+                MGB_CUDA(cudaEventRecord(ev[0], st));
+                reorder(st);
+                MGB_CUDA(cudaEventRecord(ev[1], st));
+                MGB_CUDA(cudaEventSynchronize(ev[1]));
+                MGB_CUDA(cudaEventElapsedTime(&ro, ev[0], ev[1]));
+                stage_ms[0] += ro;
+                stage_ms[8] += ro;
+            }
             iterate(st, ev);
             MGB_CUDA(cudaEventSynchronize(ev[8]));
             for (int k = 0; k < 8; ++k) {

@@ -39,6 +39,12 @@ struct TsneDev {
     uint64_t graph_kernels = 0;         // kernel nodes of the captured iteration
     std::string graph_sig;              // sizes, schedule and buffer addresses the graph was captured with
     int blocks_iter = 0, blocks_bbox = 0;
+    // spatial order of the points (the loop of a large layout): row r of every per-point array holds the caller's
+    // point perm[r]; the affinity rows and their column indices are relabelled to match. Set by reorder(),
+    // undone by set_layout / get_layout, so callers always see their own order.
+    bool permuted = false;
+    int reorder_every = 25;             // iterations between reorders (0: never)
+    DevBuf perm, perm_t, okey, ocnt, ostart, osrc, onew, olen, oip, oscan, Yt, Ut, Gt, ipt, ixt, Pt;
     ~TsneDev();
     // P must already be normalised to sum 1 (done by the caller, as magnet/tsne.py:149-150)
     void init(const int32_t* ip_h, const int32_t* ix_h, const float* P_h, int64_t n, int64_t nnz, bool host_ptrs,
@@ -50,6 +56,10 @@ struct TsneDev {
     void run(int n_iter, bool use_graph, cudaStream_t st);
     // plain launches with per-stage event timing; stage_ms[0..7] += stage times, grid[4] = last grid
     void run_profiled(int n_iter, cudaStream_t st, double* stage_ms, int* grid);
+    // sorts the points by grid box (Morton order of the boxes of the last iteration's grid), so that the rows a
+    // warp handles touch nearby nodes of the grid and nearby positions; plain launches, outside any capture
+    void reorder(cudaStream_t st);
+    bool reorder_due(int i) const;
     std::string signature() const;
     GridDesc* g() { return gdesc.as<GridDesc>(); }
 };

@@ -8,9 +8,10 @@ slots and device memory free up, and their work overlaps on the device.
   work itself is a function of the request, so the scheduler is independent of the device (it is tested on the
   host with plain functions).
 * ``FittedLayout``: the resident training data X (n, d), its layout Y (n, 2) and the kernel constants.
-  ``transform`` places new rows as the reference does: their k = n_neighbors - 1 nearest training rows (exact,
-  by blocked matmul on the device; the reference's beam search over the training graph approximates the same
-  set), smooth_knn memberships (device), the start at the membership-weighted mean of the neighbours' positions,
+  ``transform`` places new rows as the reference does: their k = n_neighbors - 1 nearest training rows by the
+  reference's beam search over the training rows' neighbour graph from the closest landmarks (on the device,
+  mg_knn_search; exact blocked matmul when no graph is given), smooth_knn memberships (device), the start at the
+  membership-weighted mean of the neighbours' positions,
   the reference's edge schedule and step scale, then the SGD with the training rows fixed (n_fixed), on the
   device. Owner mode (parallel='owner', the default here) makes a request's result a function of its inputs
   alone, so it is the same bits alone and in any mix; parallel='hogwild' agrees to float rounding. The owner
@@ -48,6 +49,9 @@ def _lib():
         lib.mg_smooth_knn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                       ctypes.c_int, ctypes.c_void_p]
         lib.mg_last_error.restype = ctypes.c_char_p
+        P_, I64 = ctypes.c_void_p, ctypes.c_int64
+        lib.mg_knn_search.argtypes = [P_, I64, ctypes.c_int, P_, P_, I64, P_, I64, P_, I64, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_uint64, ctypes.c_int, P_, P_]
         _LIB = lib
     return _LIB
 
@@ -172,7 +176,7 @@ class FittedLayout:
 
     def __init__(self, X, Y, *, a, b, rep_a=None, rep_b=1.0, n_neighbors=15, transform_epochs=100,
                  learning_rate=1.0, samples_per_node=5.0, parallel="owner", seed=0, query_block=1024,
-                 owner_chunk_edges=256):
+                 owner_chunk_edges=256, graph=None, landmarks=None, ef=None, n_entry=5):
         import torch
         self.torch = torch
         self.dev = torch.device("cuda", torch.cuda.current_device())
@@ -198,6 +202,20 @@ class FittedLayout:
         divisors = [t for t in range(8192, 1023, -1) if self.n % t == 0]
         self.tile = divisors[0] if divisors else min(4096, self.n)
         self.n_tiles = -(-self.n // self.tile)
+        # the beam search of magnet/knn.py:131-152 over the training graph, from the landmarks of
+        # choose_landmarks(n, random_state) (magnet/knn.py:125-128), ef = max(64, 2k + 10)
+        self.search = graph is not None
+        if self.search:
+            import scipy.sparse as sp
+            Gc = sp.csr_matrix(graph)
+            if landmarks is None:
+                m_l = int(min(self.n, max(100, 4 * np.sqrt(self.n))))
+                landmarks = np.sort(np.random.default_rng(self.seed).choice(self.n, m_l, replace=False))
+            self.gptr = torch.from_numpy(Gc.indptr.astype(np.int32)).to(self.dev)
+            self.gidx = torch.from_numpy(Gc.indices.astype(np.int32)).to(self.dev)
+            self.land = torch.from_numpy(np.ascontiguousarray(landmarks, dtype=np.int32)).to(self.dev)
+            self.ef = int(ef) if ef else max(64, 2 * self.k + 10)
+            self.n_entry = int(n_entry)
         # the step in units of the layout's own spacing (magnet/__init__.py:899-906): min(1, median 1-NN / 0.14)
         from scipy.spatial import cKDTree
         sub = Y[np.random.default_rng(0).choice(self.n, min(self.n, 5000), replace=False)]
@@ -208,6 +226,8 @@ class FittedLayout:
         """device bytes a transform of m rows holds at its peak: a block of query distances (and its padded copy
         when the tiles do not divide n), the first-stage top-k candidates, the neighbour arrays, the layout copy
         and the SGD's per-edge and per-node scratch"""
+        if self.search:
+            return 12 * m * self.k + 4 * m * self.d + 64 * m * self.k + 48 * (self.n + m)
         mb = min(m, self.block)
         padded = self.n_tiles * self.tile
         dist_block = 4 * mb * self.n + (4 * mb * padded if padded != self.n else 0)
@@ -248,6 +268,23 @@ class FittedLayout:
             dist[s:s + r] = torch.sqrt(torch.clamp(v + qs[s:s + r, None], min=0.0))
         return ind, dist
 
+    def beam(self, Qd):
+        """the k training rows found by the beam search for the query rows, and their distances (the square roots
+        of the squared distances, magnet/knn.py:80-83): (ind, dist) on the device"""
+        torch = self.torch
+        m = Qd.shape[0]
+        ind = torch.empty((m, self.k), dtype=torch.int32, device=self.dev)
+        d2 = torch.empty((m, self.k), dtype=torch.float32, device=self.dev)
+        rc = _lib().mg_knn_search(ctypes.c_void_p(self.Xd.data_ptr()), self.n, self.d,
+                                  ctypes.c_void_p(self.gptr.data_ptr()), ctypes.c_void_p(self.gidx.data_ptr()),
+                                  int(self.gidx.numel()), ctypes.c_void_p(self.land.data_ptr()),
+                                  int(self.land.numel()), ctypes.c_void_p(Qd.data_ptr()), m, self.k, self.ef,
+                                  self.n_entry, self.seed, -1, ctypes.c_void_p(ind.data_ptr()),
+                                  ctypes.c_void_p(d2.data_ptr()))
+        if rc != 0:
+            raise RuntimeError(_lib().mg_last_error().decode())
+        return ind.long(), torch.sqrt(torch.clamp(d2, min=0.0))
+
     def transform(self, X_new, seed=None):
         """new rows (m, d) -> their layout positions (m, 2), on this thread's stream"""
         torch = self.torch
@@ -262,7 +299,7 @@ class FittedLayout:
         with torch.cuda.stream(st):
             Q = torch.from_numpy(np.ascontiguousarray(X_new, dtype=np.float32)).to(self.dev, non_blocking=False)
             m = Q.shape[0]
-            ind, dist = self.knn(Q)
+            ind, dist = self.beam(Q) if self.search else self.knn(Q)
             vals = torch.empty_like(dist)
             rc = _lib().mg_smooth_knn(ctypes.c_void_p(dist.data_ptr()), m, self.k, self.n_neighbors, 1.0, 64,
                                       ctypes.c_void_p(vals.data_ptr()))
@@ -296,7 +333,8 @@ class FittedLayout:
 _THREAD = threading.local()
 
 
-def fit_layout(X, *, n_neighbors=15, n_epochs=200, a=None, b=None, seed=0, parallel="hogwild"):
+def fit_layout(X, *, n_neighbors=15, n_epochs=200, a=None, b=None, seed=0, parallel="hogwild",
+               return_graph=False):
     """a fit request: exact kNN, the fuzzy graph and the edge schedule, a PCA start rescaled as the reference's
     init, then the sampled SGD with 5 mid-near pairs, all device passes on this thread's stream"""
     if a is None or b is None:
@@ -309,7 +347,7 @@ def fit_layout(X, *, n_neighbors=15, n_epochs=200, a=None, b=None, seed=0, paral
     pairs = G.mid_near_pairs(X, 5, 6, seed=seed)
     D.optimize_sgd(Y, head, tail, eps, n_epochs, a=a, b=b, mid_weight=0.1, mid_pairs=pairs, graph=P, seed=seed,
                    parallel=parallel)
-    return Y
+    return (Y, P) if return_graph else Y
 
 
 def device_server(layout, slots=4, budget_fraction=0.5):

@@ -246,7 +246,7 @@ py::array_t<float> smooth_knn(py::object dist, int n_neighbors, float bandwidth,
     return out;
 }
 
-// mid_near_pairs_dense of src/nndescent.cpp:731-768 on the device (signature of src/bindings.cpp:66-67)
+// mid_near_pairs_dense of src/nndescent.cpp:731-768 on the device (signature of src/bindings.cpp:58-59)
 py::array_t<int32_t> mid_near_pairs_dense(py::object X, int n_pairs, int n_cand, uint64_t seed, int n_threads) {
     auto x = view<float>(X);
     if (x.ndim() != 2 || x.dim(1) < 1) throw std::runtime_error("X must be 2-d");
@@ -257,6 +257,23 @@ py::array_t<int32_t> mid_near_pairs_dense(py::object X, int n_pairs, int n_cand,
         check(mg_mid_near_pairs(x.ptr, n, (int)x.dim(1), n_pairs, n_cand, seed, n_threads, out.mutable_data()));
     }
     return out;
+}
+
+// knn_search of src/nndescent.cpp:660-690 on the device (signature of src/bindings.cpp:43-45)
+py::tuple knn_search(py::object X, py::object gptr, py::object gidx, py::object landmarks, py::object Q, int k, int ef,
+                     int n_entry, uint64_t seed, int n_threads) {
+    auto x = view<float>(X), q = view<float>(Q);
+    auto gp = view<int32_t>(gptr), gx = view<int32_t>(gidx), ld = view<int32_t>(landmarks);
+    if (x.ndim() != 2 || q.ndim() != 2 || x.dim(1) != q.dim(1)) throw std::runtime_error("X and Q must be 2-d with the same width");
+    const int64_t m = q.dim(0);
+    py::array_t<int32_t> oi({m, (int64_t)k});
+    py::array_t<float> od({m, (int64_t)k});
+    {
+        py::gil_scoped_release rel;
+        check(mg_knn_search(x.ptr, x.dim(0), (int)x.dim(1), gp.ptr, gx.ptr, gx.size(), ld.ptr, ld.size(), q.ptr, m, k,
+                            ef, n_entry, seed, n_threads, oi.mutable_data(), od.mutable_data()));
+    }
+    return py::make_tuple(oi, od);
 }
 
 // the fuzzy union of magnet/knn.py:221-230 on the device: (indptr, indices, data) of the n x n CSR
@@ -378,6 +395,9 @@ PYBIND11_MODULE(_native, m) {
           py::arg("n_threads") = -1);
     m.def("mid_near_pairs_dense", &mid_near_pairs_dense, "PaCMAP-style mid-near partners (dense rows, device)",
           py::arg("X"), py::arg("n_pairs") = 5, py::arg("n_cand") = 6, py::arg("seed") = 0, py::arg("n_threads") = -1);
+    m.def("knn_search", &knn_search, "Beam search of queries over a neighbour graph (dense data, device)",
+          py::arg("X"), py::arg("gptr"), py::arg("gidx"), py::arg("landmarks"), py::arg("Q"), py::arg("k"),
+          py::arg("ef") = 64, py::arg("n_entry") = 10, py::arg("seed") = 0, py::arg("n_threads") = -1);
     m.def("fuzzy_union", &fuzzy_union, "fuzzy union A + A^T - A o A^T of kNN memberships (device): (indptr, indices, data)",
           py::arg("ind"), py::arg("vals"), py::arg("n") = -1, py::arg("set_op_mix_ratio") = 1.0);
     m.def("tsne_attraction", [](py::object indptr, py::object indices, py::object data, py::object Y, float dof, int) {

@@ -16,14 +16,17 @@ def blobs(n, d, centers, seed):
     return (C[y] + rng.normal(0, 1, (n, d))).astype(np.float32), y
 
 
-def test_transform_same_alone_and_in_the_mix(mg, cuda):
+@pytest.mark.parametrize("search", ["beam", "exact"])
+def test_transform_same_alone_and_in_the_mix(mg, cuda, search):
+    """with the query kNN by beam search over the training graph (the reference's transform) and by exact
+    blocked matmul"""
     from sklearn.neighbors import KNeighborsClassifier
     from magnet_b200 import serve as S
     X, y = blobs(4600, 16, 8, seed=3)
     Xtr, ytr, Xq, yq = X[:4000], y[:4000], X[4000:], y[4000:]
-    Ytr = S.fit_layout(Xtr, n_epochs=100, seed=0)
+    Ytr, P = S.fit_layout(Xtr, n_epochs=100, seed=0, return_graph=True)
     a, b = mg.find_ab_params(1.0, 0.1)
-    layout = S.FittedLayout(Xtr, Ytr, a=a, b=b, transform_epochs=60)
+    layout = S.FittedLayout(Xtr, Ytr, a=a, b=b, transform_epochs=60, graph=P if search == "beam" else None)
     sizes = [1, 37, 200, 5, 90, 150, 64, 53]
     chunks = np.split(Xq, np.cumsum(sizes)[:-1])
 

@@ -122,3 +122,28 @@ def test_mid_spring(mg):
     expect = grad + 0.3 * (Y - Y[pairs].mean(1))
     mg.mid_spring(Y, pairs, grad, 0.3)
     assert np.allclose(grad, expect, rtol=1e-5, atol=1e-6)
+
+
+def test_spatial_reorder_keeps_the_callers_order(mg, monkeypatch):
+    """a large layout's loop sorts its points by grid box every few iterations and relabels the affinities; the
+    layout comes back in the caller's order, and matches a run without the reorder to FP32 rounding (the sums run
+    in another order)"""
+    from magnet_b200 import graph as G
+    rng = np.random.default_rng(4)
+    n = 30000
+    C = rng.normal(0, 6, (12, 16))
+    X = (C[rng.integers(0, 12, n)] + rng.normal(0, 1, (n, 16))).astype(np.float32)
+    ind, dist = G.exact_knn(X, 15)
+    P = G.fuzzy_graph(ind, dist, 15)
+    Y0 = (rng.normal(0, 1e-4, (n, 2))).astype(np.float32)
+    monkeypatch.setenv("MAGNET_TSNE_REORDER_EVERY", "0")
+    Ya = mg.optimize_tsne(P, Y0.copy(), n_iter=40, early_iter=20)
+    monkeypatch.setenv("MAGNET_TSNE_REORDER_EVERY", "10")
+    Yb = mg.optimize_tsne(P, Y0.copy(), n_iter=40, early_iter=20)
+    assert np.isfinite(Yb).all()
+    spread = float(Ya.std())
+    d = np.linalg.norm(Ya - Yb, axis=1)
+    assert np.median(d) < 1e-3 * spread and np.percentile(d, 99) < 1e-2 * spread, (np.median(d), spread)
+    import quality   # tests/golden: the blocked FP64 KL (the whole n x n matrix would not fit at this size)
+    ka, kb = quality.kl_divergence(P, Ya), quality.kl_divergence(P, Yb)
+    assert abs(ka - kb) / ka < 0.002, (ka, kb)
