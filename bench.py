@@ -225,6 +225,7 @@ def perplexity_affinities(ind, d2, perplexity=30.0, n_steps=100, tol=1e-5):
     rows = np.repeat(np.arange(n), k)
     C = sp.csr_matrix((p.ravel(), (rows, np.asarray(ind).ravel())), shape=(n, n))
     P = ((C + C.T) / (2.0 * n)).tocsr().astype(np.float32)
+    P.eliminate_zeros()        # rows whose far neighbours' weights underflow
     P.sort_indices()
     return P
 
@@ -243,8 +244,9 @@ def kl_divergence(P, Y, dof=1.0, block=4096):
         w[np.arange(w.shape[0]), np.arange(s, s + w.shape[0])] = 0.0
         Z += w.sum()
     C = P.tocoo()
-    q = (1.0 + ((Y[C.row] - Y[C.col]) ** 2).sum(-1) / dof) ** (-dof) / Z
-    return float((C.data * np.log(C.data / q)).sum())
+    keep = C.data > 0
+    q = (1.0 + ((Y[C.row[keep]] - Y[C.col[keep]]) ** 2).sum(-1) / dof) ** (-dof) / Z
+    return float((C.data[keep] * np.log(C.data[keep] / q)).sum())
 
 
 def exact_knn_cpu(X, k):
@@ -713,6 +715,35 @@ def knn_preservation(X, Y, k=15, n_query=5000, seed=0):
     return float(np.mean([len(np.intersect1d(a[i], b[i])) / k for i in range(len(q))]))
 
 
+def precision_study(Y, n_sub=10_000, seed=0):
+    """the FFT pass's error on a 10k-point subsample of a layout: the device's FP32 spread / FFT / gather with the
+    FP64 Z reduction (FFTRepulsion2D, the reference's grid rule) against the direct FP64 all-pairs sums of the same
+    points (sumQ = sum_{i != j} (1 + |y_i - y_j|^2)^-1, F_i = sum_j (1 + |y_i - y_j|^2)^-2 (y_i - y_j)), computed
+    in FP64 on the device"""
+    import torch
+    import magnet_b200 as mg
+    rng = np.random.default_rng(seed)
+    Ys = np.ascontiguousarray(Y[rng.choice(Y.shape[0], min(n_sub, Y.shape[0]), replace=False)], dtype=np.float32)
+    sq, F = mg.FFTRepulsion2D(n_interp=3)(Ys)
+    Yd = torch.from_numpy(Ys.astype(np.float64)).cuda()
+    s64 = torch.zeros((), dtype=torch.float64, device="cuda")
+    F64 = torch.zeros_like(Yd)
+    for a in range(0, Yd.shape[0], 2048):
+        diff = Yd[a:a + 2048, None, :] - Yd[None, :, :]
+        q = 1.0 / (1.0 + (diff * diff).sum(-1))
+        idx = torch.arange(a, min(a + 2048, Yd.shape[0]), device="cuda")
+        q[idx - a, idx] = 0.0
+        s64 += q.sum()
+        F64[a:a + 2048] = ((q * q)[:, :, None] * diff).sum(1)
+    s64 = float(s64)
+    F64 = F64.cpu().numpy()
+    F = np.asarray(F, dtype=np.float64)
+    return {"n": int(Ys.shape[0]), "sumQ_rel_err": float(abs(sq - s64) / s64),
+            "F_rel_rms_err": float(np.linalg.norm(F - F64) / np.linalg.norm(F64)),
+            "F_max_rel_err": float(np.abs(F - F64).max() / np.abs(F64).max()),
+            "against": "direct FP64 all-pairs sums on the device"}
+
+
 def roofline(w, gp, peak):
     """per-stage CUDA-event times of the t-SNE iteration and of the SGD epoch kernel, the dominant kernel's
     achieved GB/s against its algorithmic bytes"""
@@ -799,6 +830,56 @@ def measured_peak():
             return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
     except (OSError, KeyError, ValueError):
         return 6650.0, "6650 GB/s, an earlier copy measurement on this pool (of fallback)"
+
+
+# ----------------------------------------------------------------------------------------------- FFT pass alone
+def fft_grid_bench(n_boxes, steps, warmup, n=300_000, seed=0):
+    """The FFT pass (spread, forward rows, column convolution, inverse rows, gather + step) at a given grid: n points
+    spread uniformly over a square of n_boxes boxes of width 0.7 (so the reference's grid rule picks that grid), a
+    random symmetric affinity matrix of 8 entries per row; per-stage CUDA-event times of the device loop over
+    `steps` iterations after `warmup`, with each stage's algorithmic bytes and achieved GB/s. The small case that
+    the per-kernel ncu captures run on (about 1.3 GB on the device at 708 boxes)."""
+    import torch
+    import scipy.sparse as sp
+    import magnet_b200 as mg
+    rng = np.random.default_rng(seed)
+    side = n_boxes * 0.7 - 0.01
+    Y = rng.uniform(0, side, (n, 2)).astype(np.float32)
+    rows = np.repeat(np.arange(n), 4)
+    cols = rng.integers(0, n, rows.size)
+    P = sp.csr_matrix((np.ones(rows.size, np.float32), (rows, cols)), shape=(n, n))
+    P = (P + P.T).tocsr()
+    P.sum_duplicates()
+    P.sort_indices()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ip, ix, dd = t(P.indptr.astype(np.int32)), t(P.indices.astype(np.int32)), t((P.data / P.data.sum()).astype(np.float32))
+    Yd = t(Y)
+    if warmup:
+        mg._native.optimize_tsne_profiled(ip, ix, dd, Yd.clone(), warmup, 0, 12.0, 1.0, -1.0, 3, 0.7, 1.0)
+    prof = mg._native.optimize_tsne_profiled(ip, ix, dd, Yd.clone(), steps, 0, 12.0, 1.0, -1.0, 3, 0.7, 1.0)
+    nb, N, M, Mh = prof["grid"]
+    nnz = int(P.nnz)
+    alg = {"spread": 8.0 * n + 12.0 * N * N, "row_fwd": 12.0 * N * N + 24.0 * N * Mh,
+           "col_conv": 48.0 * N * Mh + 8.0 * M * Mh, "row_inv": 24.0 * N * Mh + 12.0 * N * N,
+           "gather_attr_step": 12.0 * N * N + 8.0 * n + 16.0 * nnz + 68.0 * n}
+    peak, src = measured_peak()
+    out = {"metric": "FFT pass stages at a fixed grid", "unit": "ms", "n_points": n, "nnz": nnz, "steps": steps,
+           "warmup": warmup, "grid": {"n_boxes": nb, "N": N, "M": M}, "peak_gbs": peak, "peak_source": src,
+           "stages": {}}
+    for k in ("bbox_grid", "twiddles", "spectra", "spread", "row_fwd", "col_conv", "row_inv", "gather_attr_step"):
+        ms = prof[k] / steps
+        st = {"ms": round(ms, 4)}
+        if k in alg:
+            st["alg_bytes"] = alg[k]
+            st["gbs"] = round(alg[k] / (ms * 1e-3) / 1e9, 1)
+            st["frac"] = round(alg[k] / (ms * 1e-3) / 1e9 / peak, 4)
+        out["stages"][k] = st
+    fp = ("spread", "row_fwd", "col_conv", "row_inv")
+    fms = sum(prof[k] for k in fp) / steps
+    fb = sum(alg[k] for k in fp)
+    out["fft_pass"] = {"ms": round(fms, 4), "alg_bytes": fb, "gbs": round(fb / (fms * 1e-3) / 1e9, 1),
+                       "frac": round(fb / (fms * 1e-3) / 1e9 / peak, 4)}
+    print(json.dumps(out))
 
 
 # ----------------------------------------------------------------------------------------------- fuzzy graph
@@ -975,12 +1056,16 @@ def reference_serve(n_requests=300, rate=200.0, fit_sizes=(5000, 20000, 50000), 
                              "server": "one request at a time in arrival order", "setup_s": round(setup_s, 1)}}
 
 
-def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 50000), seed=3):
+def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 50000), seed=3, dist=None):
     """The served form: a fitted 200k x 64 layout resident on the device; transform() requests of 1-4096 new rows
     from the same mixture with Poisson arrivals at `rate` per second (100 SGD epochs each, the training rows
     fixed), interleaved with fit requests of 5k-50k rows. Run once on one slot (the plain form: one request at a
-    time) and once on `slots` slots (continuous batching); latency is submit to result."""
+    time) and once on `slots` slots (continuous batching); latency is submit to result. With several ranks every
+    rank keeps its own resident copy of the layout, the requests are placed on the ranks by free device memory
+    (magnet_b200.replicas.place, the same placement on every rank) and each rank serves its share; the latencies
+    and placed rows are gathered, and the summary covers the whole stream."""
     from magnet_b200 import serve as S
+    from magnet_b200 import replicas as Rp
     import magnet_b200 as mg
     t0 = time.perf_counter()
     X, draw = serve_workload(seed=seed)
@@ -990,6 +1075,16 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
     setup_s = time.perf_counter() - t0
     sizes, gaps, batches, fit_at = serve_stream(draw, n_requests, rate, fit_sizes, seed)
     big = batches[int(np.argmax(sizes))]
+    # the stream in submission order: (arrival index, kind, rows) and each request's device bytes
+    stream = []
+    for i in range(n_requests):
+        stream.append((i, "transform", batches[i]))
+        if i in fit_at:
+            stream.append((i, "fit", fit_at[i]))
+    nbytes = [layout.request_bytes(len(r)) if k == "transform" else S.fit_bytes(len(r), X.shape[1])
+              for _, k, r in stream]
+    rank = 0 if dist is None else dist.get_rank()
+    owner = Rp.place(nbytes, Rp.free_bytes(dist, budget_fraction=0.5))
 
     def run(k):
         srv = S.device_server(layout, slots=k)
@@ -998,38 +1093,60 @@ def serve_bench(n_requests=300, rate=200.0, slots=4, fit_sizes=(5000, 20000, 500
         for f in warm:
             f.result()
         srv.done.clear()
-        futs, kinds = [], []
+        if dist is not None:
+            dist.barrier()
+        futs = []
         t_next = time.perf_counter()
-        for i in range(n_requests):
-            t_next += gaps[i]
+        last = -1
+        for j, (i, kind, rows) in enumerate(stream):
+            if i != last:   # the arrival of request i (a fit arrives with the transform it is keyed by)
+                t_next += gaps[i]
+                last = i
+            if owner[j] != rank:
+                continue
             dt = t_next - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
-            m = int(sizes[i])
-            futs.append(srv.submit("transform", (batches[i], i), layout.request_bytes(m), m))
-            kinds.append("transform")
-            if i in fit_at:
-                Xf = fit_at[i]
-                futs.append(srv.submit("fit", Xf, S.fit_bytes(len(Xf), X.shape[1]), len(Xf)))
-                kinds.append("fit")
-        res = [f.result() for f in futs]
+            payload = (rows, i) if kind == "transform" else rows
+            futs.append((j, kind, srv.submit(kind, payload, nbytes[j], len(rows))))
+        res = [(j, kind, f.result()) for j, kind, f in futs]
         srv.close()
-        placed = [r for r, kind in zip(res, kinds) if kind == "transform"]
-        tr = S.latency_summary(srv.done, "transform")
-        fi = S.latency_summary(srv.done, "fit")
-        tr["knn15"] = transform_knn15(X, Y, np.concatenate(batches), np.concatenate(placed))
+        recs = [(r.kind, r.t_submit, r.t_done, r.points) for r in srv.done]
+        placed = [(j, y) for j, kind, y in res if kind == "transform"]
+        if dist is not None:
+            allrecs = [None] * dist.get_world_size()
+            dist.all_gather_object(allrecs, recs)
+            recs = [r for part in allrecs for r in part]
+        placed = Rp.gather_results(placed, dist)
+        tr, fi = summarise(recs, "transform"), summarise(recs, "fit")
+        order = [j for j, (_, kind, _) in enumerate(stream) if kind == "transform"]
+        X_new = np.concatenate([stream[j][2] for j in order])
+        tr["knn15"] = transform_knn15(X, Y, X_new, np.concatenate(placed))
         return {k2: round(v, 4 if k2 == "knn15" else 2) for k2, v in tr.items()}, \
             {k2: round(v, 1) for k2, v in fi.items()}
 
     plain, plain_fit = run(1)
     mixed, mixed_fit = run(slots)
+    world = 1 if dist is None else dist.get_world_size()
     return {"transform": mixed | {"slots": slots}, "transform_plain": plain | {"slots": 1},
             "fit_requests": {"mixed": mixed_fit, "plain": plain_fit},
-            "serve_config": {"layout": "200,000 x 64, 50-Gaussian mixture, seed 3, k=15, resident",
+            "serve_config": {"layout": "200,000 x 64, 50-Gaussian mixture, seed 3, k=15, resident%s" %
+                                       (" on each of %d GPUs" % world if world > 1 else ""),
                              "requests": n_requests, "rate_per_s": rate, "batch": "uniform integer [1, 4096]",
                              "transform_epochs": 100, "fits": list(fit_sizes), "mode": "owner",
                              "query_knn": "beam search over the training graph (device)",
-                             "setup_s": round(setup_s, 1)}}
+                             "placement": "by free HBM over %d rank(s)" % world, "setup_s": round(setup_s, 1)}}
+
+
+def summarise(recs, kind):
+    """p50 / p99 / mean latency (ms) and points/s of the (kind, t_submit, t_done, points) records of one kind"""
+    rs = [r for r in recs if r[0] == kind]
+    if not rs:
+        return {}
+    lat = np.array([(r[2] - r[1]) * 1e3 for r in rs])
+    span = max(r[2] for r in rs) - min(r[1] for r in rs)
+    return {"requests": len(rs), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "points_per_s": float(sum(r[3] for r in rs) / max(span, 1e-9))}
 
 
 # ----------------------------------------------------------------------------------------------- ranks
@@ -1062,10 +1179,16 @@ def main():
     ap.add_argument("--graph", action="store_true", help="time the fuzzy neighbour graph instead of the layout")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--fft-grid", type=int, default=0, help="time the FFT pass alone at this many boxes per side")
     ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4],
                     help="1: the 10k umap layout, 2: the 70k tsne layout, 3 (default): the 1M hybrid layout, "
                          "4: 256 batched t-SNE layouts")
     args = ap.parse_args()
+    if args.fft_grid:
+        import torch
+        torch.cuda.set_device(0)
+        fft_grid_bench(args.fft_grid, args.steps, args.warmup)
+        return
     if args.config in (1, 2, 4):
         if args.impl != "reference":
             import torch
@@ -1174,13 +1297,14 @@ def main():
 
     rf = roofline(w, gp, measured_peak())
     knn15 = knn_preservation(w["X"], Y_final)
+    precision = precision_study(Y_final)
     n_gpus = world
     line = {"metric": METRIC, "value": round(seconds_per_layout(ms, n_gpus), 4), "unit": "s", "n_gpus": n_gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config,
             "inputs": {"graph": w["graph"], "edges": int(w["head"].size), "setup_s": round(w["setup_s"], 1)},
-            "knn15": round(knn15, 4), "grid": rf["grid"],
+            "knn15": round(knn15, 4), "grid": rf["grid"], "precision": precision,
             "e2e": {"value": round(seconds_per_layout(e2e_ms, n_gpus), 4), "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": rf["roofline"],
@@ -1195,7 +1319,7 @@ def main():
                                     "sample": "unavailable: %s" % e}
     if not args.no_serve:
         try:
-            line.update(serve_bench(n_requests=args.serve_requests))
+            line.update(serve_bench(n_requests=args.serve_requests, dist=dist))
         except Exception as e:  # noqa: BLE001  (the layout's line is reported either way)
             line["transform"] = {"error": "%s: %s" % (type(e).__name__, e)}
     if dist is not None:

@@ -31,6 +31,7 @@ def _load_host():
     spec = _ilu.spec_from_file_location("magnet_host_native._magnet", path)
     mod = _ilu.module_from_spec(spec)
     spec.loader.exec_module(mod)
+    _sys.modules[spec.name] = mod   # so that a later loader of the same file finds it
     return mod
 
 

@@ -531,30 +531,27 @@ void launch_list(const SgdDev& c, int blocks, const int64_t* eptr, const uint16_
     else hogwild_list_kernel<D, FAST, false, false><<<blocks, kThreads, 0, s>>>(c, eptr, cnt16, epoch, alpha, mid_w, rpt);
 }
 
-// ---------------------------------------------------------------------------------------------- flat form
+// ---------------------------------------------------------------------------------------------- range form
 // The sampled set of an epoch as one bit per edge (bit i of bits[i / 32]: eons[i] <= epoch, the test of
-// src/layout.cpp:135), one warp ballot per 32 consecutive edges; only eons is read. Block 0 also clears the row
-// counter of the sample kernel that follows on the stream.
+// src/layout.cpp:135), one warp ballot per 32 consecutive edges; only eons is read.
 __global__ void __launch_bounds__(kThreads) sample_bits_kernel(const float* __restrict__ eons, int64_t E, float fepoch,
-                                                               uint32_t* __restrict__ bits,
-                                                               unsigned long long* __restrict__ next_row) {
+                                                               uint32_t* __restrict__ bits) {
     const int lane = threadIdx.x & 31;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *next_row = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x - lane; base < E; base += stride) {
         const int64_t i = base + lane;
-        const bool s = i < E && !(eons[i] > fepoch);
-        const uint32_t m = __ballot_sync(0xffffffffu, s);
+        const bool smp = i < E && !(eons[i] > fepoch);
+        const uint32_t m = __ballot_sync(0xffffffffu, smp);
         if (lane == 0) bits[base >> 5] = m;
     }
 }
 
-// One sample of the flat form: the schedule update of its edge (eons / eonns as schedule_edge), then the sample's
-// reads and its steps. The reads that do not depend on one another (the edge's schedule state and tail, the mid-range
-// partner's index) are issued together, then the positions of the tail, the negatives and the partner.
+// One sample of the range form: the schedule update of its edge (eons / eonns as schedule_edge), then the sample's
+// reads and its steps. The reads that do not depend on one another (the edge's schedule state and tail) are issued
+// together, then the positions of the tail and the negatives.
 template <int D, bool FAST, bool REP1, bool B1>
-__device__ __forceinline__ void flat_sample(const SgdDev& c, int64_t u, int64_t i, int epoch, float fepoch, float alpha,
-                                            float mid_w, float jit, float* yu) {
+__device__ __forceinline__ void range_sample(const SgdDev& c, int64_t u, int64_t i, int epoch, float fepoch,
+                                             float alpha, float mid_w, float jit, float* yu) {
     const float eon = c.eons[i];
     const float eps = c.eps[i];
     const float eonn = c.eonns[i];
@@ -579,71 +576,62 @@ __device__ __forceinline__ void flat_sample(const SgdDev& c, int64_t u, int64_t 
     compute_sample<D, FAST, REP1, B1>(c, u, f, alpha, mid_w, jit, yu);
 }
 
-// The flat form of the sample pass: each thread takes a head row (rows are handed out in order by a counter, one
-// warp-aggregated atomic per group of threads that need a row at the same time), does the row's sampled edges in
-// edge order from the bit set, so the head's steps follow one another in registers as in the reference's loop, and
-// takes the next row when the row is done. Every trip of the loop is one sample for every active thread, so the
-// warp's threads stay converged on the sample's work whatever the rows' lengths. The schedule update of a sampled
-// edge happens here, once, in the sample that consumes it.
+// The range form of the sample pass: each thread owns a run of consecutive head rows, which is one contiguous run of
+// edges (the edges are sorted by head); it walks the run's sampled edges in edge order from the bit set, one
+// sample per trip of the loop, so a warp's threads stay converged on the sample's work; the head's steps follow
+// one another in registers as in the reference's loop, and the head's displacement lands with one atomic when the
+// thread leaves the row. The schedule update of a sampled edge happens here, once, in the sample that consumes it.
 template <int D, bool FAST, bool REP1, bool B1>
-__global__ void __launch_bounds__(kThreads, 4) hogwild_flat_kernel(SgdDev c, const int64_t* __restrict__ eptr,
-                                                                   const uint32_t* __restrict__ bits,
-                                                                   unsigned long long* __restrict__ next_row, int epoch,
-                                                                   float alpha,
-                                                                   float mid_w) {
+__global__ void __launch_bounds__(kThreads, 4) hogwild_range_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+                                                                    const uint32_t* __restrict__ bits, int epoch,
+                                                                    float alpha, float mid_w, int64_t rows_per_thread) {
     const float fepoch = (float)epoch;
     const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
-    const int lane = threadIdx.x & 31;
-    int64_t u = -1, pos = 0, e1 = 0;
+    const int64_t u0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * rows_per_thread;
+    if (u0 >= c.n) return;
+    const int64_t u1 = u0 + rows_per_thread < c.n ? u0 + rows_per_thread : c.n;
+    int64_t pos = eptr[u0];
+    const int64_t end = eptr[u1];
+    int64_t u = u0, row_end = eptr[u0 + 1];
     float yu[D], y0[D];
     bool have = false;
     for (;;) {
         int64_t i = -1;
-        for (;;) {
-            if (u >= 0) {
-                while (pos < e1) {
-                    const int64_t wend = (pos | 31) + 1;
-                    uint32_t m = bits[pos >> 5] & (0xffffffffu << (pos & 31));
-                    if (e1 < wend) m &= (1u << (e1 & 31)) - 1u;
-                    if (m) { i = (pos & ~(int64_t)31) + __ffs(m) - 1; pos = i + 1; break; }
-                    pos = wend;
-                }
-                if (i >= 0) break;
-                if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
-                have = false;
-            }
-            // the next row for every thread of the warp that needs one
-            const unsigned act = __activemask();
-            const int leader = __ffs(act) - 1;
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(next_row, (unsigned long long)__popc(act));
-            base = __shfl_sync(act, base, leader);
-            const int64_t r = (int64_t)base + __popc(act & ((1u << lane) - 1u));
-            if (r >= c.n) { u = -1; break; }
-            u = r;
-            pos = eptr[u];
-            e1 = eptr[u + 1];
+        while (pos < end) {
+            const int64_t wend = (pos | 31) + 1;
+            uint32_t m = bits[pos >> 5] & (0xffffffffu << (pos & 31));
+            if (end < wend) m &= (1u << (end & 31)) - 1u;
+            if (m) { i = (pos & ~(int64_t)31) + __ffs(m) - 1; pos = i + 1; break; }
+            pos = wend;
         }
-        if (u < 0) break;
+        if (i < 0) break;
+        if (i >= row_end) {   // the sample is in a later row: the current one is done
+            if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+            have = false;
+            do { ++u; row_end = eptr[u + 1]; } while (i >= row_end);
+        }
         if (!have) {
             load_pos<D>(c.Y, u, yu);
 #pragma unroll
             for (int d = 0; d < D; ++d) y0[d] = yu[d];
             have = true;
         }
-        flat_sample<D, FAST, REP1, B1>(c, u, i, epoch, fepoch, alpha, mid_w, jit, yu);
+        range_sample<D, FAST, REP1, B1>(c, u, i, epoch, fepoch, alpha, mid_w, jit, yu);
     }
+    if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
 }
 
 template <int D, bool FAST>
-void launch_flat(const SgdDev& c, int blocks, const int64_t* eptr, const uint32_t* bits, unsigned long long* next_row,
-                 int epoch,
-                 float alpha, float mid_w, cudaStream_t s) {
+void launch_range(const SgdDev& c, int blocks, const int64_t* eptr, const uint32_t* bits, int epoch, float alpha,
+                  float mid_w, cudaStream_t s) {
+    const int64_t threads = (int64_t)blocks * kThreads;
+    const int64_t rpt = (c.n + threads - 1) / threads;
+    blocks = (int)((c.n + rpt * kThreads - 1) / (rpt * kThreads));
     const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
-    if (rep1 && b1) hogwild_flat_kernel<D, FAST, true, true><<<blocks, kThreads, 0, s>>>(c, eptr, bits, next_row, epoch, alpha, mid_w);
-    else if (rep1) hogwild_flat_kernel<D, FAST, true, false><<<blocks, kThreads, 0, s>>>(c, eptr, bits, next_row, epoch, alpha, mid_w);
-    else if (b1) hogwild_flat_kernel<D, FAST, false, true><<<blocks, kThreads, 0, s>>>(c, eptr, bits, next_row, epoch, alpha, mid_w);
-    else hogwild_flat_kernel<D, FAST, false, false><<<blocks, kThreads, 0, s>>>(c, eptr, bits, next_row, epoch, alpha, mid_w);
+    if (rep1 && b1) hogwild_range_kernel<D, FAST, true, true><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
+    else if (rep1) hogwild_range_kernel<D, FAST, true, false><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
+    else if (b1) hogwild_range_kernel<D, FAST, false, true><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
+    else hogwild_range_kernel<D, FAST, false, false><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
 }
 
 // Row kernel (any dim, any loss): one thread owns a head row and walks it in order with counter draws.
@@ -877,14 +865,12 @@ void hogwild_epoch(const SgdDev& c, SgdWork& w, const int64_t* eptr, int epoch, 
     const int form = env_int("MGB_SGD_FORM", 1);
     if (form == 1 && eptr && c.loss == 0 && (D == 2 || D == 3)) {
         uint32_t* bits = w.samp.as<uint32_t>();
-        auto* next_row = static_cast<unsigned long long*>(w.ctr.ensure(sizeof(unsigned long long)));
-        sample_bits_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c.eons, c.n_edges, (float)epoch,
-                                                                                     bits, next_row);
+        sample_bits_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c.eons, c.n_edges, (float)epoch, bits);
         MGB_LAUNCH_CHECK();
-        const int blocks = (int)std::min<int64_t>((c.n + kThreads - 1) / kThreads, (cap + kThreads - 1) / kThreads);
+        const int blocks = (int)std::min<int64_t>(blocks_for(c.n, kThreads, 8), (cap + kThreads - 1) / kThreads);
         constexpr int DD = D == 0 ? 2 : D;
-        if (c.kernel == 0 && !c.node_b) launch_flat<DD, true>(c, blocks, eptr, bits, next_row, epoch, alpha, mid_w, s);
-        else launch_flat<DD, false>(c, blocks, eptr, bits, next_row, epoch, alpha, mid_w, s);
+        if (c.kernel == 0 && !c.node_b) launch_range<DD, true>(c, blocks, eptr, bits, epoch, alpha, mid_w, s);
+        else launch_range<DD, false>(c, blocks, eptr, bits, epoch, alpha, mid_w, s);
     } else if (eptr && c.loss == 0 && (D == 2 || D == 3)) {
         uint16_t* cnt16 = w.samp.as<uint16_t>();
         schedule16_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c, epoch, cnt16);

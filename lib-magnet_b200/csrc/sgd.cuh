@@ -34,7 +34,6 @@ struct SgdDev {
 struct SgdWork {
     DevBuf cnt, state, delta, eptr, flag;
     DevBuf samp;               // the epoch's sampled set (counter mode fast path)
-    DevBuf ctr;                // row counter of the flat sample kernel
     // owner mode: node rows, chunk bounds, per-edge negatives, per-node stream states, marked chunks, snapshots
     DevBuf o_row, o_own, o_neg, o_state, o_dirty, o_snap, o_snap_m, o_snap_v, o_snap_t;
 };

@@ -1,11 +1,11 @@
 #!/usr/bin/env bash
 # Builds the reference's own native module (kerighan/lib-magnet src/*.cpp, pybind11) from the sources
 # where they lie, into oracle/_ref/. Used only as a test oracle and as the timed CPU baseline.
-# Needs the reference checkout (default /root/reference, override with MAGNET_REFERENCE_DIR); on a machine
+# Needs the reference checkout (MAGNET_REFERENCE_DIR, else the folder `reference` beside the repository); on a machine
 # without it the prebuilt oracle/_ref/ module is used as it is.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${MAGNET_REFERENCE_DIR:-/root/reference}"
+REF="${MAGNET_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 SUFFIX="$(python3-config --extension-suffix 2>/dev/null || python3 -c 'import sysconfig;print(sysconfig.get_config_var("EXT_SUFFIX"))')"
 TARGET="$OUT/_magnet$SUFFIX"

@@ -122,6 +122,7 @@ def reference():
         spec = importlib.util.spec_from_file_location("magnet_reference_native._magnet", cands[0])
         mod = importlib.util.module_from_spec(spec)
         spec.loader.exec_module(mod)
+        sys.modules[spec.name] = mod   # visible to other loaders of the same file in this process
         _ref = mod
     return _ref
 

@@ -1,6 +1,6 @@
 """Generates the golden fixtures of tests/golden/ from the reference itself (kerighan/lib-magnet 3.0.2).
 
-Runs only where the reference checkout is available (default /root/reference, override with
+Runs only where the reference checkout is available (the folder `reference` beside this repository, override with
 MAGNET_REFERENCE_DIR) and its native module has been compiled by oracle/build_ref.sh. Every output is produced
 by the reference's own code: its compiled `_magnet` (optimize_layout at n_threads=1 and in owner mode, FFTConv2D,
 tsne_attraction, tsne_step, bbox_2d, smooth_knn) and its Python drivers (magnet/tsne.py FFTRepulsion2D /
@@ -16,7 +16,7 @@ import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("MAGNET_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("MAGNET_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))   # the compiled reference module, importable as _magnet
 sys.path.insert(0, REF)
 sys.path.insert(0, HERE)

@@ -47,7 +47,8 @@ def kl_divergence(P, Y, dof=1.0, block=2048):
         w[np.arange(w.shape[0]), np.arange(s, s + w.shape[0])] = 0.0
         Z += w.sum()
     C = P.tocoo()
-    d2 = ((Y[C.row] - Y[C.col]) ** 2).sum(-1)
+    keep = C.data > 0          # zero entries contribute nothing (0 log 0 = 0)
+    d2 = ((Y[C.row[keep]] - Y[C.col[keep]]) ** 2).sum(-1)
     q = (1.0 + d2 / dof) ** (-dof) / Z
-    p = C.data
+    p = C.data[keep]
     return float((p * np.log(p / q)).sum())
