@@ -83,11 +83,9 @@ struct BlockSync {
 __device__ __forceinline__ float chan(const float4& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
 
 // ------------------------------------------------------------------------------------------------ spread
-// One thread per point, nodes accumulated with vector float atomics. Lanes whose points share a box first reduce
-// the node values: the whole warp with shuffles (the dense case: early-exaggeration layouts put everything in a few
-// boxes), or, when every group of lanes sharing a box is a run of consecutive lanes (points sorted by box, as the
-// loop's spatial order leaves them), each run with a segmented shuffle reduction, so the run's first lane issues
-// one atomic per node and no two lanes of a warp instruction hit the same node.
+// One thread per point, nodes accumulated with vector float atomics. Warps whose 32 points share one box (the
+// dense case: early-exaggeration layouts put everything in a few boxes) first reduce the node values with
+// shuffles, so one atomic per node replaces 32.
 template <int NI>
 __global__ void __launch_bounds__(256) spread_kernel(const float2* __restrict__ Y, int64_t n,
                                                      const GridDesc* __restrict__ gd, float4* __restrict__ W,
@@ -106,9 +104,6 @@ __global__ void __launch_bounds__(256) spread_kernel(const float2* __restrict__ 
         locate<NI>(x, y, xmin, ymin, width, inv_w, nb, bx, by, wx, wy);
         const int key = act ? bx * nb + by : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
-        const unsigned run = peers >> (__ffs(peers) - 1);
-        const bool runs = __all_sync(0xffffffffu, (run & (run + 1u)) == 0u);     // every group consecutive lanes
-        const bool shared = __any_sync(0xffffffffu, act && __popc(peers) > 1);
         if (peers == 0xffffffffu && key >= 0) {
             // whole warp in one box: reduce per node, lane q issues node q
 #pragma unroll
@@ -124,28 +119,6 @@ __global__ void __launch_bounds__(256) spread_kernel(const float2* __restrict__ 
                         s2 += __shfl_xor_sync(0xffffffffu, s2, o);
                     }
                     if (lane == ((a * NI + b) & 31)) {
-                        const int gx = bx * NI + a, gy = by * NI + b;
-                        atomicAdd(&W[(size_t)gx * pitch + gy], make_float4(s0, s1, s2, 0.f));
-                    }
-                }
-            }
-        } else if (runs && shared) {
-            // runs of lanes in one box: each lane adds the lanes after it in its run, doubling the reach
-            const bool first = act && (lane == 0 || ((peers >> (lane - 1)) & 1u) == 0u);
-#pragma unroll
-            for (int a = 0; a < NI; ++a) {
-#pragma unroll
-                for (int b = 0; b < NI; ++b) {
-                    const float w = act ? wx[a] * wy[b] : 0.f;
-                    float s0 = w, s1 = w * x, s2 = w * y;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const float t0 = __shfl_down_sync(0xffffffffu, s0, o);
-                        const float t1 = __shfl_down_sync(0xffffffffu, s1, o);
-                        const float t2 = __shfl_down_sync(0xffffffffu, s2, o);
-                        if (lane + o < 32 && ((peers >> (lane + o)) & 1u)) { s0 += t0; s1 += t1; s2 += t2; }
-                    }
-                    if (first) {
                         const int gx = bx * NI + a, gy = by * NI + b;
                         atomicAdd(&W[(size_t)gx * pitch + gy], make_float4(s0, s1, s2, 0.f));
                     }

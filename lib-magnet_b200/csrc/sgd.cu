@@ -374,9 +374,6 @@ struct Fetched {
     float yv[D];
     int32_t k[kNegBatch];
     float yk[kNegBatch][D];
-    int32_t w;         // mid-range partner read ahead (w >= 0), none this sample (-1), or left to compute (-2)
-    float yw[D];
-    uint32_t kmask;    // range form: bit q set when negative q is drawn and is not the head (k[] unused)
 };
 
 template <int D>
@@ -385,7 +382,6 @@ __device__ __forceinline__ void fetch_sample(const SgdDev& c, int64_t i, int nn,
     f.nn = nn;
     f.v = c.tail[i];
     f.key = sample_key(stream_seed(c.seed, epoch, (uint64_t)i));
-    f.w = -2;
     load_pos<D>(c.Y, f.v, f.yv);
 #pragma unroll
     for (int q = 0; q < kNegBatch; ++q) {
@@ -420,7 +416,7 @@ __device__ __forceinline__ void add_negative(const SgdDev& c, int64_t u, const f
 
 // One sample: the steps of epoch_worker (src/layout.cpp:145-256) in the reference's order (attraction and the
 // tail's step, negatives, mid-range partner, the head's step) with counter draws.
-template <int D, bool FAST, bool REP1, bool B1, bool KMASK = false>
+template <int D, bool FAST, bool REP1, bool B1>
 __device__ __forceinline__ void compute_sample(const SgdDev& c, int64_t u, const Fetched<D>& f, float alpha,
                                                float mid_w, float jit, float* yu) {
     float gu[D];
@@ -447,10 +443,8 @@ __device__ __forceinline__ void compute_sample(const SgdDev& c, int64_t u, const
         }
     }
 #pragma unroll
-    for (int q = 0; q < kNegBatch; ++q) {
-        const bool use = KMASK ? ((f.kmask >> q) & 1u) != 0u : (f.k[q] >= 0 && f.k[q] != (int32_t)u);
-        if (use) add_negative<D, FAST, REP1>(c, u, yu, f.yk[q], f.key, q, jit, gu);
-    }
+    for (int q = 0; q < kNegBatch; ++q)
+        if (f.k[q] >= 0 && f.k[q] != (int32_t)u) add_negative<D, FAST, REP1>(c, u, yu, f.yk[q], f.key, q, jit, gu);
     for (int p = kNegBatch; p < f.nn; ++p) {   // rare: more negatives than one batch
         const int32_t k = (int32_t)below_of(counter_draw(f.key, p), (uint32_t)c.n);
         if (k == (int32_t)u) continue;
@@ -458,15 +452,7 @@ __device__ __forceinline__ void compute_sample(const SgdDev& c, int64_t u, const
         load_pos<D>(c.Y, k, yk);
         add_negative<D, FAST, REP1>(c, u, yu, yk, f.key, p, jit, gu);
     }
-    if (mid_w > 0.0f && f.w >= 0) {
-        // the partner and its position were read with the sample's other inputs (mid-near pairs)
-        if (f.w != (int32_t)u) {
-            float gk[D];
-#pragma unroll
-            for (int d = 0; d < D; ++d) { const float g = -mid_w * (yu[d] - f.yw[d]); gu[d] += g; gk[d] = -g; }
-            if (f.w >= c.n_fixed) HogwildSink().template apply<D>(c, f.w, gk, alpha, D);
-        }
-    } else if (mid_w > 0.0f && f.w == -2) {
+    if (mid_w > 0.0f) {
         CounterDraws dr(f.key);
         if (uniform_of(dr.mid()) < c.mid_rate) {
             const int32_t w = mid_partner(c, (int32_t)u, f.v, dr);
@@ -560,13 +546,12 @@ __global__ void __launch_bounds__(kThreads) sample_bits_kernel(const float* __re
     }
 }
 
-// The reads of one sample of the range form, after the schedule update of its edge (eons / eonns as schedule_edge):
-// the edge's schedule state and tail, then the positions of the tail and the negatives and, with mid-near pairs,
-// the sample's mid-range draws (draws 1024 and 1025, as mid_partner takes them) and the partner's position. None of
-// them depends on the head's position, so they are issued before the previous sample of the thread is computed.
-template <int D>
-__device__ __forceinline__ void range_fetch(const SgdDev& c, int64_t u, int64_t i, int epoch, float fepoch,
-                                            float mid_w, Fetched<D>& f) {
+// One sample of the range form: the schedule update of its edge (eons / eonns as schedule_edge), then the sample's
+// reads and its steps. The reads that do not depend on one another (the edge's schedule state and tail) are issued
+// together, then the positions of the tail and the negatives.
+template <int D, bool FAST, bool REP1, bool B1>
+__device__ __forceinline__ void range_sample(const SgdDev& c, int64_t u, int64_t i, int epoch, float fepoch,
+                                             float alpha, float mid_w, float jit, float* yu) {
     const float eon = c.eons[i];
     const float eps = c.eps[i];
     const float eonn = c.eonns[i];
@@ -577,28 +562,18 @@ __device__ __forceinline__ void range_fetch(const SgdDev& c, int64_t u, int64_t 
     c.eons[i] = __fadd_rn(eon, eps);
     c.eonns[i] = __fadd_rn(eonn, __fmul_rn((float)nn, epn));
     nn = nn > 0 ? nn : 0;
+    Fetched<D> f;
     f.i = i;
     f.nn = nn;
     f.v = v;
     f.key = key;
     load_pos<D>(c.Y, v, f.yv);
-    f.kmask = 0u;
 #pragma unroll
     for (int q = 0; q < kNegBatch; ++q) {
-        if (q < nn) {
-            const int32_t k = (int32_t)below_of(counter_draw(key, q), (uint32_t)c.n);
-            load_pos<D>(c.Y, k, f.yk[q]);
-            if (k != (int32_t)u) f.kmask |= 1u << q;
-        }
+        f.k[q] = q < nn ? (int32_t)below_of(counter_draw(key, q), (uint32_t)c.n) : -1;
+        if (f.k[q] >= 0) load_pos<D>(c.Y, f.k[q], f.yk[q]);
     }
-    f.w = -2;
-    if (mid_w > 0.0f && c.mid_pairs && !c.jump_indptr) {
-        f.w = -1;
-        if (uniform_of(counter_draw(key, kMidDraw)) < c.mid_rate) {
-            f.w = c.mid_pairs[u * c.n_mid + below_of(counter_draw(key, kMidDraw + 1), (uint32_t)c.n_mid)];
-            load_pos<D>(c.Y, f.w, f.yw);
-        }
-    }
+    compute_sample<D, FAST, REP1, B1>(c, u, f, alpha, mid_w, jit, yu);
 }
 
 // The range form of the sample pass: each thread owns a run of consecutive head rows, which is one contiguous run of
@@ -606,8 +581,8 @@ __device__ __forceinline__ void range_fetch(const SgdDev& c, int64_t u, int64_t 
 // sample per trip of the loop, so a warp's threads stay converged on the sample's work; the head's steps follow
 // one another in registers as in the reference's loop, and the head's displacement lands with one atomic when the
 // thread leaves the row. The schedule update of a sampled edge happens here, once, in the sample that consumes it.
-template <int D, bool FAST, bool REP1, bool B1, int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) hogwild_range_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+template <int D, bool FAST, bool REP1, bool B1>
+__global__ void __launch_bounds__(kThreads, 4) hogwild_range_kernel(SgdDev c, const int64_t* __restrict__ eptr,
                                                                     const uint32_t* __restrict__ bits, int epoch,
                                                                     float alpha, float mid_w, int64_t rows_per_thread) {
     const float fepoch = (float)epoch;
@@ -617,73 +592,64 @@ __global__ void __launch_bounds__(kThreads, MINB) hogwild_range_kernel(SgdDev c,
     const int64_t u1 = u0 + rows_per_thread < c.n ? u0 + rows_per_thread : c.n;
     int64_t pos = eptr[u0];
     const int64_t end = eptr[u1];
-    // the next sampled edge of the thread's run, or -1
-    auto next = [&]() -> int64_t {
+    int64_t u = u0, row_end = eptr[u0 + 1];
+    float yu[D], y0[D];
+    bool have = false;
+    for (;;) {
+        int64_t i = -1;
         while (pos < end) {
             const int64_t wend = (pos | 31) + 1;
             uint32_t m = bits[pos >> 5] & (0xffffffffu << (pos & 31));
             if (end < wend) m &= (1u << (end & 31)) - 1u;
-            if (m) { const int64_t i = (pos & ~(int64_t)31) + __ffs(m) - 1; pos = i + 1; return i; }
+            if (m) { i = (pos & ~(int64_t)31) + __ffs(m) - 1; pos = i + 1; break; }
             pos = wend;
         }
-        return -1;
-    };
-    int64_t i = next();
-    if (i < 0) return;
-    int64_t u = u0, row_end = eptr[u0 + 1];
-    while (i >= row_end) { ++u; row_end = eptr[u + 1]; }
-    Fetched<D> f;
-    range_fetch<D>(c, u, i, epoch, fepoch, mid_w, f);
-    float yu[D], y0[D];
-    load_pos<D>(c.Y, u, yu);
-#pragma unroll
-    for (int d = 0; d < D; ++d) y0[d] = yu[d];
-    for (;;) {
-        // the next sample's reads go out before this one is computed
-        const int64_t j = next();
-        int64_t uj = u, rj = row_end;
-        Fetched<D> g;
-        if (j >= 0) {
-            while (j >= rj) { ++uj; rj = eptr[uj + 1]; }
-            range_fetch<D>(c, uj, j, epoch, fepoch, mid_w, g);
+        if (i < 0) break;
+        if (i >= row_end) {   // the sample is in a later row: the current one is done
+            if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+            have = false;
+            do { ++u; row_end = eptr[u + 1]; } while (i >= row_end);
         }
-        compute_sample<D, FAST, REP1, B1, true>(c, u, f, alpha, mid_w, jit, yu);
-        if (j < 0) break;
-        if (uj != u) {   // the head's row is done: its displacement lands with one atomic
-            if (u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
-            u = uj;
-            row_end = rj;
+        if (!have) {
             load_pos<D>(c.Y, u, yu);
 #pragma unroll
             for (int d = 0; d < D; ++d) y0[d] = yu[d];
+            have = true;
         }
-        f = g;
+        range_sample<D, FAST, REP1, B1>(c, u, i, epoch, fepoch, alpha, mid_w, jit, yu);
     }
-    if (u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+    if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
 }
 
-template <int D, bool FAST, int MINB>
-void launch_range_b(const SgdDev& c, int blocks, const int64_t* eptr, const uint32_t* bits, int epoch, float alpha,
-                    float mid_w, cudaStream_t s) {
+// Blocks of a kernel the device holds at once (the SM count times the blocks one SM holds); the same on every
+// B200, so it is asked once per kernel.
+template <typename K>
+int resident_blocks(K kernel) {
+    static const int count = [kernel] {
+        int dev = 0, sms = 0, per_sm = 0;
+        MGB_CUDA(cudaGetDevice(&dev));
+        MGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        MGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+        return std::max(1, sms * per_sm);
+    }();
+    return count;
+}
+
+// The grid of the range form never exceeds what the device holds resident: the rows are split into static runs, so
+// a second wave of blocks would run alone after the first.
+template <int D, bool FAST>
+void launch_range(const SgdDev& c, int blocks, const int64_t* eptr, const uint32_t* bits, int epoch, float alpha,
+                  float mid_w, cudaStream_t s) {
+    const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
+    auto kernel = rep1 && b1 ? hogwild_range_kernel<D, FAST, true, true>
+                : rep1       ? hogwild_range_kernel<D, FAST, true, false>
+                : b1         ? hogwild_range_kernel<D, FAST, false, true>
+                             : hogwild_range_kernel<D, FAST, false, false>;
+    blocks = std::max(1, std::min(blocks, resident_blocks(kernel)));
     const int64_t threads = (int64_t)blocks * kThreads;
     const int64_t rpt = (c.n + threads - 1) / threads;
     blocks = (int)((c.n + rpt * kThreads - 1) / (rpt * kThreads));
-    const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
-    if (rep1 && b1) hogwild_range_kernel<D, FAST, true, true, MINB><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
-    else if (rep1) hogwild_range_kernel<D, FAST, true, false, MINB><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
-    else if (b1) hogwild_range_kernel<D, FAST, false, true, MINB><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
-    else hogwild_range_kernel<D, FAST, false, false, MINB><<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
-}
-
-// blocks: resident blocks at most (minb per SM), so no partial second wave idles the device
-template <int D, bool FAST>
-void launch_range(const SgdDev& c, int64_t cap, int minb, const int64_t* eptr, const uint32_t* bits, int epoch,
-                  float alpha, float mid_w, cudaStream_t s) {
-    const int blocks = (int)std::min<int64_t>(std::min<int64_t>(blocks_for(c.n, kThreads, minb),
-                                                                (cap + kThreads - 1) / kThreads),
-                                              (int64_t)minb * kNumSMs);
-    if (minb == 2) launch_range_b<D, FAST, 2>(c, blocks, eptr, bits, epoch, alpha, mid_w, s);
-    else launch_range_b<D, FAST, 3>(c, blocks, eptr, bits, epoch, alpha, mid_w, s);
+    kernel<<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
 }
 
 // Row kernel (any dim, any loss): one thread owns a head row and walks it in order with counter draws.
@@ -919,10 +885,10 @@ void hogwild_epoch(const SgdDev& c, SgdWork& w, const int64_t* eptr, int epoch, 
         uint32_t* bits = w.samp.as<uint32_t>();
         sample_bits_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c.eons, c.n_edges, (float)epoch, bits);
         MGB_LAUNCH_CHECK();
-        const int minb = env_int("MGB_SGD_MINB", 3) == 2 ? 2 : 3;
+        const int blocks = (int)std::min<int64_t>(blocks_for(c.n, kThreads, 8), (cap + kThreads - 1) / kThreads);
         constexpr int DD = D == 0 ? 2 : D;
-        if (c.kernel == 0 && !c.node_b) launch_range<DD, true>(c, cap, minb, eptr, bits, epoch, alpha, mid_w, s);
-        else launch_range<DD, false>(c, cap, minb, eptr, bits, epoch, alpha, mid_w, s);
+        if (c.kernel == 0 && !c.node_b) launch_range<DD, true>(c, blocks, eptr, bits, epoch, alpha, mid_w, s);
+        else launch_range<DD, false>(c, blocks, eptr, bits, epoch, alpha, mid_w, s);
     } else if (eptr && c.loss == 0 && (D == 2 || D == 3)) {
         uint16_t* cnt16 = w.samp.as<uint16_t>();
         schedule16_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c, epoch, cnt16);

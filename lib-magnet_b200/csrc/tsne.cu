@@ -637,9 +637,10 @@ void TsneDev::init(const int32_t* ip_h, const int32_t* ix_h, const float* P_h, i
     require(s.min_boxes >= 1 && s.max_boxes >= s.min_boxes, "invalid box limits");
     n = n_; nnz = nnz_; ni = s.ni; sch = s; dof = dof_;
     permuted = false;   // the affinities are copied afresh below, in the caller's order
-    // MAGNET_TSNE_REORDER_EVERY: iterations between spatial reorders (0 turns them off)
+    // MAGNET_TSNE_REORDER_EVERY: iterations between spatial reorders (0, the default, turns them off: sorted
+    // points make a warp's spread atomics collide on the same nodes, which costs what the gather gains)
     if (const char* v = std::getenv("MAGNET_TSNE_REORDER_EVERY")) reorder_every = std::max(0, std::atoi(v));
-    else reorder_every = 25;
+    else reorder_every = 0;
     if (threads_per_row <= 0) {
         const double deg = n > 0 ? (double)nnz / (double)n : 0.0;
         tpr = deg < 3 ? 1 : deg < 6 ? 2 : deg < 12 ? 4 : deg < 40 ? 8 : deg < 100 ? 16 : 32;

