@@ -109,7 +109,7 @@ __device__ __forceinline__ double middle2_dispatch(int R, const fft3::Plan& p, f
 // One (column, channel) per work item, one shared-memory buffer per block: the three channels' convolutions are
 // independent (channel 0 also yields the column's Z share), so a block holds a single transform and the SM
 // holds more blocks to overlap one block's barriers with another's stages.
-constexpr int kColBlocks = 4;   // 4 x 64 registers x 256 threads; 4 buffers of M = 6000 fit the SM
+constexpr int kColBlocks = 3;   // 3 x 80 registers x 256 threads; 3 buffers of M = 6000 fit the SM
 
 __global__ void __launch_bounds__(kColThreads, kColBlocks) col3_kernel(GridDesc* __restrict__ gd,
                                                               const fft3::Plan* __restrict__ plans,
@@ -226,7 +226,7 @@ struct PhiStore {
 
 // Forward row transforms of the 3 charge channels, separated into the half spectra of the 4 rows and written
 // transposed (WhT[c][k][g]); the consumed rows of W are zeroed for the next spread.
-__global__ void __launch_bounds__(kRowThreads, 3) row_fwd3_kernel(const GridDesc* __restrict__ gd,
+__global__ void __launch_bounds__(kRowThreads, 2) row_fwd3_kernel(const GridDesc* __restrict__ gd,
                                                                   const fft3::Plan* __restrict__ plans,
                                                                   float4* __restrict__ W, int pitchW,
                                                                   float2* __restrict__ WhT, int Np, int Mhmax,
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) row_fwd3_kernel(const GridDesc
 // Inverse row transforms of the potential channels 1-3: each pair rebuilt from the two half spectra (Hermitian
 // extension, DC and Nyquist imaginary parts dropped as a c2r does) straight into the digit-reversed positions
 // the inverse stages start from, transformed, scaled by 1/M^2 (src/fftconv.cpp:176, 188-198).
-__global__ void __launch_bounds__(kRowThreads, 3) row_inv3_kernel(const GridDesc* __restrict__ gd,
+__global__ void __launch_bounds__(kRowThreads, 2) row_inv3_kernel(const GridDesc* __restrict__ gd,
                                                                   const fft3::Plan* __restrict__ plans,
                                                                   const float2* __restrict__ PhT, int Np, int Mhmax,
                                                                   float* __restrict__ phi, int pitchP,

@@ -621,6 +621,100 @@ __global__ void __launch_bounds__(kThreads, 4) hogwild_range_kernel(SgdDev c, co
     if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
 }
 
+// ---------------------------------------------------------------------------------------------- split form
+// The range form with the samples, not the rows, split evenly: thread t of T takes the samples of ranks
+// [t S / T, (t + 1) S / T) of the epoch's S sampled edges, in edge order. A thread still walks consecutive edges,
+// so a head's steps follow one another in its registers; a row cut between two threads is held by both, and each
+// lands its own displacement with an atomic when it leaves the row. The sampled set is the same bit set, counted
+// per chunk of kChunkWords words so that a thread finds its first sample by a binary search of the chunks' prefix
+// sums and a walk of one chunk.
+constexpr int kChunkWords = 64;   // 2048 edges per chunk
+
+__global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64_t* __restrict__ off, int64_t* total);
+
+// the bit set as sample_bits_kernel, one warp per chunk, and the chunk's count of sampled edges; words past the
+// last edge are written as 0, so every chunk is whole
+__global__ void __launch_bounds__(kThreads) chunk_bits_kernel(const float* __restrict__ eons, int64_t E, float fepoch,
+                                                              int64_t n_chunks, uint32_t* __restrict__ bits,
+                                                              int32_t* __restrict__ count) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t ch = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < n_chunks; ch += warps) {
+        const int64_t base = ch * (kChunkWords * 32);
+        int total = 0;
+#pragma unroll 1
+        for (int w0 = 0; w0 < kChunkWords; w0 += 8) {
+            bool smp[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int64_t i = base + (int64_t)(w0 + q) * 32 + lane;
+                smp[q] = i < E && !(eons[i] > fepoch);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t m = __ballot_sync(0xffffffffu, smp[q]);
+                total += __popc(m);
+                if (lane == q) bits[ch * kChunkWords + w0 + q] = m;
+            }
+        }
+        if (lane == 0) count[ch] = total;
+    }
+}
+
+template <int D, bool FAST, bool REP1, bool B1>
+__global__ void __launch_bounds__(kThreads, 4) hogwild_split_kernel(SgdDev c, const int64_t* __restrict__ eptr,
+                                                                    const uint32_t* __restrict__ bits,
+                                                                    const int64_t* __restrict__ cpre, int64_t n_chunks,
+                                                                    int epoch, float alpha, float mid_w) {
+    const float fepoch = (float)epoch;
+    const float jit = 1e-3f / fmaxf(alpha, 1e-6f);
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t S = cpre[n_chunks];
+    const int64_t r0 = t * S / T, r1 = (t + 1) * S / T;
+    if (r0 >= r1) return;
+    // the chunk holding the sample of rank r0: the last chunk whose prefix is <= r0 (it has a sample past r0)
+    int64_t lo = 0, hi = n_chunks;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (cpre[mid] <= r0) lo = mid; else hi = mid;
+    }
+    int64_t k = r0 - cpre[lo];
+    int64_t w = lo * kChunkWords;
+    const int64_t w_end = n_chunks * kChunkWords;
+    uint32_t m = bits[w];
+    while (k >= __popc(m) && w + 1 < w_end) { k -= __popc(m); m = bits[++w]; }
+    for (int j = 0; j < (int)k; ++j) m &= m - 1u;
+    if (m == 0u) return;   // counts and bits disagree: cannot happen, both come from one ballot
+    int64_t pos = w * 32 + __ffs(m) - 1;
+    const int64_t end = c.n_edges;
+    int64_t u = c.head[pos], row_end = eptr[u + 1];
+    float yu[D], y0[D];
+    bool have = false;
+    for (int64_t left = r1 - r0; left > 0; --left) {
+        int64_t i = -1;
+        while (pos < end) {
+            const uint32_t mm = bits[pos >> 5] & (0xffffffffu << (pos & 31));
+            if (mm) { i = (pos & ~(int64_t)31) + __ffs(mm) - 1; pos = i + 1; break; }
+            pos = (pos | 31) + 1;
+        }
+        if (i < 0 || i >= end) break;
+        if (i >= row_end) {
+            if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+            have = false;
+            do { ++u; row_end = eptr[u + 1]; } while (i >= row_end);
+        }
+        if (!have) {
+            load_pos<D>(c.Y, u, yu);
+#pragma unroll
+            for (int d = 0; d < D; ++d) y0[d] = yu[d];
+            have = true;
+        }
+        range_sample<D, FAST, REP1, B1>(c, u, i, epoch, fepoch, alpha, mid_w, jit, yu);
+    }
+    if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
+}
+
 // Blocks of a kernel the device holds at once (the SM count times the blocks one SM holds); the same on every
 // B200, so it is asked once per kernel.
 template <typename K>
@@ -650,6 +744,24 @@ void launch_range(const SgdDev& c, int blocks, const int64_t* eptr, const uint32
     const int64_t rpt = (c.n + threads - 1) / threads;
     blocks = (int)((c.n + rpt * kThreads - 1) / (rpt * kThreads));
     kernel<<<blocks, kThreads, 0, s>>>(c, eptr, bits, epoch, alpha, mid_w, rpt);
+}
+
+template <int D, bool FAST>
+void launch_split(const SgdDev& c, int64_t threads, const int64_t* eptr, uint32_t* bits, int32_t* count, int64_t* cpre,
+                  int64_t n_chunks, int epoch, float alpha, float mid_w, cudaStream_t s) {
+    chunk_bits_kernel<<<blocks_for(n_chunks * 32, kThreads, 8), kThreads, 0, s>>>(c.eons, c.n_edges, (float)epoch,
+                                                                                  n_chunks, bits, count);
+    MGB_LAUNCH_CHECK();
+    offsets_kernel<<<1, 1024, 0, s>>>(count, n_chunks, cpre, cpre + n_chunks);
+    MGB_LAUNCH_CHECK();
+    const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
+    auto kernel = rep1 && b1 ? hogwild_split_kernel<D, FAST, true, true>
+                : rep1       ? hogwild_split_kernel<D, FAST, true, false>
+                : b1         ? hogwild_split_kernel<D, FAST, false, true>
+                             : hogwild_split_kernel<D, FAST, false, false>;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((threads + kThreads - 1) / kThreads,
+                                                                  resident_blocks(kernel)));
+    kernel<<<blocks, kThreads, 0, s>>>(c, eptr, bits, cpre, n_chunks, epoch, alpha, mid_w);
 }
 
 // Row kernel (any dim, any loss): one thread owns a head row and walks it in order with counter draws.
@@ -880,8 +992,16 @@ template <int D>
 void hogwild_epoch(const SgdDev& c, SgdWork& w, const int64_t* eptr, int epoch, float alpha, float mid_w,
                    cudaStream_t s) {
     const int64_t cap = max_in_flight(c);
-    const int form = env_int("MGB_SGD_FORM", 1);
-    if (form == 1 && eptr && c.loss == 0 && (D == 2 || D == 3)) {
+    const int form = env_int("MGB_SGD_FORM", 2);
+    if (form == 2 && eptr && c.loss == 0 && (D == 2 || D == 3)) {
+        const int64_t n_chunks = std::max<int64_t>(1, (c.n_edges + kChunkWords * 32 - 1) / (kChunkWords * 32));
+        uint32_t* bits = w.samp.as<uint32_t>();
+        int64_t* cpre = reinterpret_cast<int64_t*>(bits + n_chunks * kChunkWords);
+        int32_t* count = reinterpret_cast<int32_t*>(cpre + n_chunks + 1);
+        constexpr int DD = D == 0 ? 2 : D;
+        if (c.kernel == 0 && !c.node_b) launch_split<DD, true>(c, cap, eptr, bits, count, cpre, n_chunks, epoch, alpha, mid_w, s);
+        else launch_split<DD, false>(c, cap, eptr, bits, count, cpre, n_chunks, epoch, alpha, mid_w, s);
+    } else if (form == 1 && eptr && c.loss == 0 && (D == 2 || D == 3)) {
         uint32_t* bits = w.samp.as<uint32_t>();
         sample_bits_kernel<<<blocks_for(c.n_edges, kThreads, 8), kThreads, 0, s>>>(c.eons, c.n_edges, (float)epoch, bits);
         MGB_LAUNCH_CHECK();
@@ -963,9 +1083,12 @@ void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha
     const int64_t* eptr = row_pointers(c, w, s);
     if (stream_mode == 0) {
         if (eptr && c.loss == 0 && (c.dim == 2 || c.dim == 3)) {
-            // the list form's u16 per edge, or the flat form's bit per edge (rounded up to whole words)
+            // the list form's u16 per edge, or the range forms' bit per edge (whole chunks of 2048 edges), the
+            // chunks' prefix sums and counts
+            const size_t n_chunks = (size_t)std::max<int64_t>(1, (c.n_edges + kChunkWords * 32 - 1) / (kChunkWords * 32));
             w.samp.ensure(std::max<size_t>(sizeof(uint16_t) * std::max<int64_t>(c.n_edges, 1),
-                                           sizeof(uint32_t) * ((c.n_edges + 31) / 32 + 1)));
+                                           sizeof(uint32_t) * n_chunks * kChunkWords + sizeof(int64_t) * (n_chunks + 1) +
+                                               sizeof(int32_t) * n_chunks));
         }
         for (int e = e0; e < e1; ++e) {
             float alpha, mid_w;
