@@ -25,6 +25,8 @@
 #include <cmath>
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
+#include <unordered_map>
 
 namespace mgb {
 
@@ -661,7 +663,18 @@ __global__ void __launch_bounds__(kThreads) chunk_bits_kernel(const float* __res
     }
 }
 
-template <int D, bool FAST, bool REP1, bool B1>
+// The edge arrays of the 32 edges of bit-set word w (one 128-byte line of each) brought into L2 ahead of use: a
+// thread's samples walk its edges in order, so the line of word w + 2 is needed a dozen samples later.
+__device__ __forceinline__ void prefetch_edges(const SgdDev& c, int64_t w) {
+    const int64_t e = w * 32;
+    if (e >= c.n_edges) return;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c.eons + e));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c.eps + e));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c.eonns + e));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c.tail + e));
+}
+
+template <int D, bool FAST, bool REP1, bool B1, bool PF>
 __global__ void __launch_bounds__(kThreads, 4) hogwild_split_kernel(SgdDev c, const int64_t* __restrict__ eptr,
                                                                     const uint32_t* __restrict__ bits,
                                                                     const int64_t* __restrict__ cpre, int64_t n_chunks,
@@ -689,6 +702,8 @@ __global__ void __launch_bounds__(kThreads, 4) hogwild_split_kernel(SgdDev c, co
     int64_t pos = w * 32 + __ffs(m) - 1;
     const int64_t end = c.n_edges;
     int64_t u = c.head[pos], row_end = eptr[u + 1];
+    int64_t seen = w;   // the last word whose look-ahead line went out
+    if (PF) { prefetch_edges(c, w + 1); prefetch_edges(c, w + 2); }
     float yu[D], y0[D];
     bool have = false;
     for (int64_t left = r1 - r0; left > 0; --left) {
@@ -699,6 +714,10 @@ __global__ void __launch_bounds__(kThreads, 4) hogwild_split_kernel(SgdDev c, co
             pos = (pos | 31) + 1;
         }
         if (i < 0 || i >= end) break;
+        if (PF && (i >> 5) > seen) {
+            seen = i >> 5;
+            prefetch_edges(c, seen + 2);
+        }
         if (i >= row_end) {
             if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
             have = false;
@@ -719,15 +738,21 @@ __global__ void __launch_bounds__(kThreads, 4) hogwild_split_kernel(SgdDev c, co
 // B200, so it is asked once per kernel.
 template <typename K>
 int resident_blocks(K kernel) {
-    static const int count = [kernel] {
-        int dev = 0, sms = 0, per_sm = 0;
-        MGB_CUDA(cudaGetDevice(&dev));
-        MGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        MGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
-        return std::max(1, sms * per_sm);
-    }();
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> known;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto it = known.find(reinterpret_cast<const void*>(kernel));
+    if (it != known.end()) return it->second;
+    int dev = 0, sms = 0, per_sm = 0;
+    MGB_CUDA(cudaGetDevice(&dev));
+    MGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+    const int count = std::max(1, sms * per_sm);
+    known.emplace(reinterpret_cast<const void*>(kernel), count);
     return count;
 }
+
+int env_int(const char* name, int dflt);
 
 // The grid of the range form never exceeds what the device holds resident: the rows are split into static runs, so
 // a second wave of blocks would run alone after the first.
@@ -755,10 +780,11 @@ void launch_split(const SgdDev& c, int64_t threads, const int64_t* eptr, uint32_
     offsets_kernel<<<1, 1024, 0, s>>>(count, n_chunks, cpre, cpre + n_chunks);
     MGB_LAUNCH_CHECK();
     const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
-    auto kernel = rep1 && b1 ? hogwild_split_kernel<D, FAST, true, true>
-                : rep1       ? hogwild_split_kernel<D, FAST, true, false>
-                : b1         ? hogwild_split_kernel<D, FAST, false, true>
-                             : hogwild_split_kernel<D, FAST, false, false>;
+    const bool pf = env_int("MGB_SGD_PREFETCH", 1) != 0;
+    auto kernel = rep1 && b1 ? (pf ? hogwild_split_kernel<D, FAST, true, true, true> : hogwild_split_kernel<D, FAST, true, true, false>)
+                : rep1       ? (pf ? hogwild_split_kernel<D, FAST, true, false, true> : hogwild_split_kernel<D, FAST, true, false, false>)
+                : b1         ? (pf ? hogwild_split_kernel<D, FAST, false, true, true> : hogwild_split_kernel<D, FAST, false, true, false>)
+                             : (pf ? hogwild_split_kernel<D, FAST, false, false, true> : hogwild_split_kernel<D, FAST, false, false, false>);
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((threads + kThreads - 1) / kThreads,
                                                                   resident_blocks(kernel)));
     kernel<<<blocks, kThreads, 0, s>>>(c, eptr, bits, cpre, n_chunks, epoch, alpha, mid_w);
