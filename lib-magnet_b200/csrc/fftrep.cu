@@ -87,19 +87,15 @@ __device__ __forceinline__ float chan(const float4& v, int c) { return c == 0 ? 
 // dense case: early-exaggeration layouts put everything in a few boxes) first reduce the node values with
 // shuffles, so one atomic per node replaces 32.
 template <int NI>
-// With seg > 0 the points are taken in interleaved order: lane l of a warp takes point l * seg + base / 32, so the
-// 32 points of one atomic instruction lie n / 32 apart. Points sorted by box (the loop's spatial order) would
-// otherwise put a warp's 32 stencils on the same few nodes, and their atomics would serialise.
 __global__ void __launch_bounds__(256) spread_kernel(const float2* __restrict__ Y, int64_t n,
                                                      const GridDesc* __restrict__ gd, float4* __restrict__ W,
-                                                     int pitch, int64_t seg) {
+                                                     int pitch) {
     const float xmin = gd->xmin, ymin = gd->ymin, width = gd->width, inv_w = gd->inv_width;
     const int nb = gd->n_boxes;
     const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t total = seg > 0 ? 32 * seg : n;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < total; base += stride) {
-        const int64_t i = seg > 0 ? lane * seg + (base >> 5) : base + lane;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int64_t i = base + lane;
         const bool act = i < n;
         float x = 0.f, y = 0.f;
         if (act) { const float2 p = Y[i]; x = p.x; y = p.y; }
@@ -446,9 +442,9 @@ void set_smem_attr(const void* fn, size_t bytes) {
 }
 
 template <int NI>
-void spread_t(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, bool interleave, cudaStream_t s) {
+void spread_t(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, cudaStream_t s) {
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 16 * kNumSMs));
-    spread_kernel<NI><<<blocks, 256, 0, s>>>(Y, n, g, b.W.as<float4>(), b.Nmax, interleave ? (n + 31) / 32 : 0);
+    spread_kernel<NI><<<blocks, 256, 0, s>>>(Y, n, g, b.W.as<float4>(), b.Nmax);
 }
 template <int NI>
 void gather_t(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, float2* F, cudaStream_t s) {
@@ -476,8 +472,8 @@ void rep_set_grid_host(GridDesc* g_dev, float xmin, float ymin, float width, int
         default: F<8>(__VA_ARGS__); break;          \
     }
 
-void rep_spread(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, cudaStream_t s, bool interleave) {
-    MGB_NI_DISPATCH(b.ni, spread_t, Y, n, g, b, interleave, s);
+void rep_spread(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, cudaStream_t s) {
+    MGB_NI_DISPATCH(b.ni, spread_t, Y, n, g, b, s);
     MGB_LAUNCH_CHECK();
 }
 

@@ -51,8 +51,7 @@ int next_fft_len(int target);
 // kernel launches (all asynchronous on stream s; sizes read from the device GridDesc g)
 void rep_set_grid_host(GridDesc* g_dev, float xmin, float ymin, float width, int n_boxes, int ni, int M,
                        cudaStream_t s);
-// interleave: take the points in interleaved order (for points sorted by box; see spread_kernel)
-void rep_spread(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, cudaStream_t s, bool interleave = false);
+void rep_spread(const float2* Y, int64_t n, GridDesc* g, RepBuffers& b, cudaStream_t s);
 void rep_prepare_device_spectra(RepBuffers& b);   // before capture: scratch of the spectrum generation
 void rep_update_spectra(GridDesc* g, RepBuffers& b, float dof, cudaStream_t s);
 void rep_convolve(GridDesc* g, RepBuffers& b, int64_t n, cudaStream_t s, cudaEvent_t* ev = nullptr);

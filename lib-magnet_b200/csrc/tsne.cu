@@ -747,8 +747,7 @@ void TsneDev::iterate(cudaStream_t st, cudaEvent_t* ev) {
     mark(2);
     rep_update_spectra(g(), rb, dof, st);
     mark(3);
-    // with the spatial reorder on, the points are sorted by box for most of the run: spread them interleaved
-    rep_spread(Ycur.as<float2>(), n, g(), rb, st, reorder_every > 0 && n >= kReorderMinPoints);
+    rep_spread(Ycur.as<float2>(), n, g(), rb, st);
     mark(4);
     rep_convolve(g(), rb, n, st, ev ? ev + 5 : nullptr);
     switch (ni) {
