@@ -809,9 +809,9 @@ def roofline(w, gp, peak):
 
 
 def measured_traffic(stage, n):
-    """DRAM bytes per launch of a stage from the committed ncu summary (profiles/dram_traffic_hybrid_300k.md),
+    """DRAM bytes per launch of a stage from the committed ncu summary (profiles/dram_traffic_hybrid_1m.md),
     scaled to this run's size; None when the stage was not captured"""
-    path = os.path.join(ROOT, "profiles", "dram_traffic_hybrid_300k.md")
+    path = os.path.join(ROOT, "profiles", "dram_traffic_hybrid_1m.md")
     try:
         text = open(path).read()
     except OSError:

@@ -847,7 +847,9 @@ int64_t max_in_flight(const SgdDev& c) {
     return std::max<int64_t>(64, c.n / div);
 }
 
-// Threads of the split form, each holding one head at a time: n / 4, at most 81,920 (2.2 blocks of 256 per SM).
+// Threads of the split form, each holding one head at a time: n / 4 (n / 8 with Adam, whose per-node moments take
+// the concurrent steps of every thread that holds the node: at n / 4 a 600-point Adam layout lost 20 points of
+// neighbourhood purity), at most 81,920 (2.2 blocks of 256 per SM).
 // Measured on B200 (ms per epoch; 15-NN preservation of the finished layout unchanged within 0.002):
 // 1M points 0.485 at 83k threads, 0.51 at 125k, 0.53 at 167k; the 10k-point umap pass 53 ms at
 // n / 4, 94 ms at n / 8, 152 ms at n / 16 for 500 epochs. MGB_SGD_INFLIGHT_DIV = k sets n / k instead.
@@ -855,7 +857,7 @@ constexpr int64_t kSplitMaxThreads = 81920;
 int64_t split_threads(const SgdDev& c) {
     const int div = env_int("MGB_SGD_INFLIGHT_DIV", 0);
     if (div > 0) return std::max<int64_t>(64, c.n / div);
-    return std::max<int64_t>(64, std::min<int64_t>(c.n / 4, kSplitMaxThreads));
+    return std::max<int64_t>(64, std::min<int64_t>(c.n / (c.optimizer == 1 ? 8 : 4), kSplitMaxThreads));
 }
 
 template <int D>

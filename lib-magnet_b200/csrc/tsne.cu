@@ -271,14 +271,32 @@ __global__ void __launch_bounds__(kThreads) loop_iter_kernel(const float2* __res
         }
         float2 u = make_float2(0.f, 0.f), gn = make_float2(0.f, 0.f);
         if (lg == 0) { u = U[i]; gn = G[i]; }
+        // the row's entries in batches of kBatch per lane: every column index of a batch is read before any
+        // neighbour position, so a lane waits for two round trips per batch instead of two per entry (each lane
+        // still sums its entries in order)
+        constexpr int kBatch = 4;
         float ax = 0.f, ay = 0.f;
         const int32_t e1 = ip[i + 1];
-#pragma unroll 4
-        for (int32_t e = ip[i] + lg; e < e1; e += T) {
-            const float2 yj = __ldg(&Ycur[ix[e]]);
-            const float dx = yi.x - yj.x, dy = yi.y - yj.y;
-            const float w = P[e] / (1.f + (dx * dx + dy * dy) * s.inv_dof);
-            ax += w * dx; ay += w * dy;
+        for (int32_t eb = ip[i] + lg; eb < e1; eb += kBatch * T) {
+            int32_t jj[kBatch];
+            float pp[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const int32_t e = eb + q * T;
+                jj[q] = e < e1 ? __ldg(&ix[e]) : -1;
+                pp[q] = e < e1 ? __ldg(&P[e]) : 0.f;
+            }
+            float2 yj[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) yj[q] = jj[q] >= 0 ? __ldg(&Ycur[jj[q]]) : yi;
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                if (jj[q] >= 0) {
+                    const float dx = yi.x - yj[q].x, dy = yi.y - yj[q].y;
+                    const float w = pp[q] / (1.f + (dx * dx + dy * dy) * s.inv_dof);
+                    ax += w * dx; ay += w * dy;
+                }
+            }
         }
 #pragma unroll
         for (int o = T / 2; o > 0; o >>= 1) {
