@@ -208,6 +208,17 @@ int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* sampled, int
  * log2(n_neighbors) * bandwidth in n_iter steps at most. */
 int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter, float* out);
 
+/* The edge schedule of MAGNET.transform (magnet/__init__.py:907-912, with _sampling_frequencies of
+ * magnet/__init__.py:51-66), on the device: w (m, k) memberships of m new rows and ind (m, k) their neighbours
+ * among n_train fixed rows -> the kept edges in row order, head[e] = n_train + row, tail[e] = ind, eps[e] = 1 / freq,
+ * with freq = min(1, s w) summing to samples_per_node * m and kept when freq >= 1 / n_epochs; *n_kept (host) their
+ * count. head, tail and eps are device arrays of m * k entries. s is solved in FP64 (bisection, then exactly on
+ * its segment), so eps can differ from the host's sorted cumulative sum by FP64 rounding only. Synchronises the
+ * stream. */
+int mg_transform_schedule(const float* w, const int64_t* ind, int64_t m, int k, int64_t n_train,
+                          double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                          int64_t* n_kept);
+
 /* mid_near_pairs_dense (src/nndescent.cpp:731-768, bound at src/bindings.cpp:58-59): X (n, d) dense rows -> out
  * (n, n_pairs), for every row and pair the second closest, by squared distance then index, of n_cand rows drawn
  * at random (the row itself replaced by the next row). The draws are the reference's streams for n_threads threads

@@ -679,6 +679,23 @@ extern "C" int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbor
     });
 }
 
+extern "C" int mg_transform_schedule(const float* w, const int64_t* ind, int64_t m, int k, int64_t n_train,
+                                     double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                                     int64_t* n_kept) {
+    return guard([&] {
+        require(m >= 0 && k >= 1 && n_train >= 0 && n_kept, "need m >= 0, k >= 1, n_train >= 0 and n_kept");
+        require(n_epochs >= 1 && samples_per_node > 0.0, "need n_epochs >= 1 and samples_per_node > 0");
+        require(n_train + m <= INT32_MAX, "node indices must fit 32 bits");
+        const int64_t n = m * (int64_t)k;
+        if (n > 0)
+            for (const void* p : {(const void*)w, (const void*)ind, (const void*)head, (const void*)tail,
+                                  (const void*)eps})
+                require(p && is_device_ptr(p), "w, ind, head, tail and eps must be device arrays of m * k entries");
+        *n_kept = n == 0 ? 0 : transform_schedule_dev(w, ind, m, k, n_train, samples_per_node, n_epochs, head,
+                                                      tail, eps, graph_work(), current_stream());
+    });
+}
+
 extern "C" int mg_mid_near_pairs(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed,
                                  int n_threads, int32_t* out) {
     return guard([&] {

@@ -349,6 +349,109 @@ __global__ void narrow_kernel(const int64_t* __restrict__ in, int64_t n, int32_t
         out[i] = (int32_t)in[i];
 }
 
+// ------------------------------------------------------------------------------------------------ transform schedule
+// The edge schedule of MAGNET.transform (magnet/__init__.py:907-912) for m new rows of k neighbours, one block:
+// freq_i = min(1, s w_i) with s such that sum(freq) = samples_per_node * m (magnet/__init__.py:51-66), the edges with
+// freq >= 1 / n_epochs kept in row order with head n_train + row, their neighbour as tail and eps = 1 / freq.
+// The reference sorts the weights and walks the breakpoints of the piecewise-linear sum; here s is bracketed by
+// bisection in FP64 until the bracket is a few ulps wide, then solved exactly on the segment the bracket lies
+// in: s = (target - k) / (sum of the unsaturated weights), k the weights saturated at the bracket. Sums are FP64
+// block reductions in a fixed order, so the result is the same from call to call; it differs from the host's
+// sorted cumulative sum only by FP64 rounding.
+constexpr int kSchedThreads = 1024;
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    return t;
+}
+
+__global__ void __launch_bounds__(kSchedThreads) transform_schedule_kernel(
+    const float* __restrict__ w, const int64_t* __restrict__ ind, int64_t n, int k, int64_t n_train, double target,
+    double min_freq, int32_t* __restrict__ head, int32_t* __restrict__ tail, float* __restrict__ eps,
+    int64_t* __restrict__ n_kept) {
+    __shared__ double red[kSchedThreads / 32];
+    __shared__ int64_t scan[kSchedThreads / 32];
+    __shared__ int64_t carry;
+    // sum, positive count, smallest positive weight
+    double sum = 0.0, npos = 0.0, wmin = 1e300;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = (double)w[i];
+        sum += v;
+        if (v > 0.0) { npos += 1.0; wmin = fmin(wmin, v); }
+    }
+    sum = block_sum_d(sum, red);
+    npos = block_sum_d(npos, red);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wmin = fmin(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = wmin;
+    __syncthreads();
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) wmin = fmin(wmin, red[i]);
+    // s: all ones when n <= target (the reference returns ones, zero weights included); saturating every positive
+    // weight when they are too few (the reference's s = 1 / max(w_min, 1e-300)); else the exact solution
+    bool ones = (double)n <= target;
+    double s = 0.0;
+    if (!ones && npos <= target) {
+        s = 1e300;
+    } else if (!ones) {
+        double lo = target / sum, hi = 1.0 / wmin;
+        for (int it = 0; it < 200 && hi > lo * (1.0 + 4e-16); ++it) {
+            const double mid = 0.5 * (lo + hi);
+            double f = 0.0;
+            for (int64_t i = threadIdx.x; i < n; i += blockDim.x) f += fmin(1.0, mid * (double)w[i]);
+            f = block_sum_d(f, red);
+            if (f < target) lo = mid; else hi = mid;
+        }
+        double cnt = 0.0, rest = 0.0;
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const double v = (double)w[i];
+            if (lo * v > 1.0) cnt += 1.0; else rest += v;
+        }
+        cnt = block_sum_d(cnt, red);
+        rest = block_sum_d(rest, red);
+        s = rest > 0.0 ? (target - cnt) / rest : hi;
+    }
+    // the kept edges in row order: a block-wide exclusive scan of the keep flags, 1024 edges at a time
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t base = 0; base < n; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        double freq = 0.0;
+        bool keep = false;
+        if (i < n) {
+            freq = ones ? 1.0 : fmin(1.0, s * (double)w[i]);
+            keep = freq >= min_freq;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) scan[warp] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t acc = 0;
+            for (int j = 0; j < (int)(blockDim.x >> 5); ++j) { const int64_t t = scan[j]; scan[j] = acc; acc += t; }
+            red[0] = (double)acc;   // this tile's count
+        }
+        __syncthreads();
+        if (keep) {
+            const int64_t pos = carry + scan[warp] + __popc(bal & ((1u << lane) - 1u));
+            head[pos] = (int32_t)(n_train + i / k);
+            tail[pos] = (int32_t)ind[i];
+            eps[pos] = (float)(1.0 / freq);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += (int64_t)red[0];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *n_kept = carry;
+}
+
 }  // namespace
 
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, DevBuf& tmp, cudaStream_t s) {
@@ -426,6 +529,20 @@ int64_t fuzzy_union_dev(const int32_t* ind, const float* vals, int64_t n_rows, i
     MGB_LAUNCH_CHECK();
     MGB_CUDA(cudaStreamSynchronize(s));
     return nnz;
+}
+
+int64_t transform_schedule_dev(const float* w, const int64_t* ind, int64_t m, int k, int64_t n_train,
+                               double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                               GraphWork& gw, cudaStream_t s) {
+    const int64_t n = m * (int64_t)k;
+    int64_t* cnt = static_cast<int64_t*>(gw.sched.ensure(sizeof(int64_t)));
+    transform_schedule_kernel<<<1, kSchedThreads, 0, s>>>(w, ind, n, k, n_train, samples_per_node * (double)m,
+                                                          1.0 / (double)n_epochs, head, tail, eps, cnt);
+    MGB_LAUNCH_CHECK();
+    int64_t kept = 0;
+    MGB_CUDA(cudaMemcpyAsync(&kept, cnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    MGB_CUDA(cudaStreamSynchronize(s));
+    return kept;
 }
 
 }  // namespace mgb

@@ -9,6 +9,7 @@ namespace mgb {
 struct GraphWork {
     DevBuf sigma, rho, part, acol, aval, alen, tcnt, tptr, tcur, trow, tval, ucnt, uptr, scan, flag;
     DevBuf mid_state, mid_tab;   // mid-near partners: per-row stream states, jump tables and chunk tables
+    DevBuf sched;                // the transform schedule's kept-edge count
 };
 
 // memberships (n_rows, k) of sorted neighbour distances; `target` = log2(n_neighbors) * bandwidth, computed by the
@@ -27,6 +28,13 @@ int64_t fuzzy_union_dev(const int32_t* ind, const float* vals, int64_t n_rows, i
 // threads (>= 1) and its squared-distance kernel `order` (0 AVX-512, 1 AVX2, 2 plain loop).
 void mid_near_pairs_dev(const float* X, int64_t n, int d, int n_pairs, int n_cand, uint64_t seed, int n_threads,
                         int order, int32_t* out, GraphWork& w, cudaStream_t s);
+// The edge schedule of MAGNET.transform (magnet/__init__.py:907-912) for memberships w (m, k) of m new rows and
+// their neighbours ind (m, k): the kept edges in row order as (head = n_train + row, tail, eps = 1 / freq), with
+// freq = min(1, s w) summing to samples_per_node * m and kept when freq >= 1 / n_epochs. head, tail and eps hold
+// m * k entries; returns the number kept (synchronises s).
+int64_t transform_schedule_dev(const float* w, const int64_t* ind, int64_t m, int k, int64_t n_train,
+                               double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                               GraphWork& gw, cudaStream_t s);
 // out[0..n] = exclusive scan of in[0..n) and, in out[n], the total (tmp: tile sums)
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, DevBuf& tmp, cudaStream_t s);
 // knn_search (src/nndescent.cpp:585-690): the beam search of queries Q (m, d) over the training rows X (n, d) and

@@ -461,15 +461,14 @@ __device__ __forceinline__ void compute_sample(const SgdDev& c, int64_t u, const
 template <int D, bool FAST, bool REP1, bool B1>
 __device__ __forceinline__ void range_sample(const SgdDev& c, int64_t u, int64_t i, int epoch, float fepoch,
                                              float alpha, float mid_w, float jit, float* yu) {
-    const float eon = c.eons[i];
-    const float eps = c.eps[i];
-    const float eonn = c.eonns[i];
-    const int32_t v = c.tail[i];
+    const float2 eo = c.eo[i];
+    const EdgeRO te = c.te[i];
+    const float eon = eo.x, eonn = eo.y, eps = te.eps;
+    const int32_t v = te.tail;
     const uint32_t key = sample_key(stream_seed(c.seed, epoch, (uint64_t)i));
     const float epn = eps / c.negative_sample_rate;
     int nn = (int)((fepoch - eonn) / epn);
-    c.eons[i] = __fadd_rn(eon, eps);
-    c.eonns[i] = __fadd_rn(eonn, __fmul_rn((float)nn, epn));
+    c.eo[i] = make_float2(__fadd_rn(eon, eps), __fadd_rn(eonn, __fmul_rn((float)nn, epn)));
     nn = nn > 0 ? nn : 0;
     Fetched<D> f;
     f.i = i;
@@ -500,7 +499,7 @@ __global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64
 
 // the bit set (bit i of bits[i / 32] set when edge i is sampled), one warp ballot per 32 edges and one warp per
 // chunk, and the chunk's count of sampled edges; words past the last edge are written as 0, so every chunk is whole
-__global__ void __launch_bounds__(kThreads) chunk_bits_kernel(const float* __restrict__ eons, int64_t E, float fepoch,
+__global__ void __launch_bounds__(kThreads) chunk_bits_kernel(const float2* __restrict__ eo, int64_t E, float fepoch,
                                                               int64_t n_chunks, uint32_t* __restrict__ bits,
                                                               int32_t* __restrict__ count) {
     const int lane = threadIdx.x & 31;
@@ -514,7 +513,7 @@ __global__ void __launch_bounds__(kThreads) chunk_bits_kernel(const float* __res
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const int64_t i = base + (int64_t)(w0 + q) * 32 + lane;
-                smp[q] = i < E && !(eons[i] > fepoch);
+                smp[q] = i < E && !(eo[i].x > fepoch);
             }
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -581,6 +580,26 @@ __global__ void __launch_bounds__(kThreads, 4) hogwild_split_kernel(SgdDev c, co
     if (have && u >= c.n_fixed) flush_head<D>(c, u, D, yu, y0);
 }
 
+// The split form's packed copies of the edge fields, made at the start of a call and (eons, eonns) written back at
+// its end; a sample then reads two records instead of four arrays and writes one.
+__global__ void pack_edges_kernel(const float* __restrict__ eons, const float* __restrict__ eonns,
+                                  const int32_t* __restrict__ tail, const float* __restrict__ eps, int64_t E,
+                                  float2* __restrict__ eo, EdgeRO* __restrict__ te) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x) {
+        eo[i] = make_float2(eons[i], eonns[i]);
+        te[i] = EdgeRO{tail[i], eps[i]};
+    }
+}
+
+__global__ void unpack_edges_kernel(const float2* __restrict__ eo, int64_t E, float* __restrict__ eons,
+                                    float* __restrict__ eonns) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = eo[i];
+        eons[i] = v.x;
+        eonns[i] = v.y;
+    }
+}
+
 // Blocks of a kernel the device holds at once (the SM count times the blocks one SM holds), asked once per kernel.
 // The split form's grid stays within it, so that no block waits for a second wave.
 template <typename K>
@@ -604,7 +623,7 @@ int env_int(const char* name, int dflt);
 template <int D, bool FAST>
 void launch_split(const SgdDev& c, int64_t threads, const int64_t* eptr, uint32_t* bits, int32_t* count, int64_t* cpre,
                   int64_t n_chunks, int epoch, float alpha, float mid_w, cudaStream_t s) {
-    chunk_bits_kernel<<<blocks_for(n_chunks * 32, kThreads, 8), kThreads, 0, s>>>(c.eons, c.n_edges, (float)epoch,
+    chunk_bits_kernel<<<blocks_for(n_chunks * 32, kThreads, 8), kThreads, 0, s>>>(c.eo, c.n_edges, (float)epoch,
                                                                                   n_chunks, bits, count);
     MGB_LAUNCH_CHECK();
     offsets_kernel<<<1, 1024, 0, s>>>(count, n_chunks, cpre, cpre + n_chunks);
@@ -864,7 +883,7 @@ template <int D>
 void hogwild_epoch(const SgdDev& c, SgdWork& w, const int64_t* eptr, int epoch, float alpha, float mid_w,
                    cudaStream_t s) {
     const int64_t cap = max_in_flight(c);
-    if (eptr && c.loss == 0 && (D == 2 || D == 3)) {
+    if (c.eo && eptr && c.loss == 0 && (D == 2 || D == 3)) {
         const int64_t n_chunks = std::max<int64_t>(1, (c.n_edges + kChunkWords * 32 - 1) / (kChunkWords * 32));
         uint32_t* bits = w.samp.as<uint32_t>();
         int64_t* cpre = reinterpret_cast<int64_t*>(bits + n_chunks * kChunkWords);
@@ -938,16 +957,29 @@ void sgd_run(SgdDev& c, SgdWork& w, int stream_mode, int e0, int e1, float alpha
              float mid_w1, cudaStream_t s) {
     const int64_t* eptr = row_pointers(c, w, s);
     if (stream_mode == 0) {
-        if (eptr && c.loss == 0 && (c.dim == 2 || c.dim == 3)) {
-            // the split form's bit per edge (whole chunks of 2048 edges), the chunks' prefix sums and counts
+        SgdDev cc = c;
+        const bool split = eptr && c.loss == 0 && (c.dim == 2 || c.dim == 3) && c.n_edges > 0 && e1 > e0;
+        if (split) {
+            // the split form's bit per edge (whole chunks of 2048 edges), the chunks' prefix sums and counts, and
+            // the packed edge fields
             const size_t n_chunks = (size_t)std::max<int64_t>(1, (c.n_edges + kChunkWords * 32 - 1) / (kChunkWords * 32));
             w.samp.ensure(sizeof(uint32_t) * n_chunks * kChunkWords + sizeof(int64_t) * (n_chunks + 1) +
                           sizeof(int32_t) * n_chunks);
+            char* pk = static_cast<char*>(w.pack.ensure((sizeof(float2) + sizeof(EdgeRO)) * (size_t)c.n_edges));
+            cc.eo = reinterpret_cast<float2*>(pk);
+            cc.te = reinterpret_cast<const EdgeRO*>(pk + sizeof(float2) * (size_t)c.n_edges);
+            pack_edges_kernel<<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(
+                c.eons, c.eonns, c.tail, c.eps, c.n_edges, cc.eo, const_cast<EdgeRO*>(cc.te));
+            MGB_LAUNCH_CHECK();
         }
         for (int e = e0; e < e1; ++e) {
             float alpha, mid_w;
-            sgd_sched(c, e, e0, e1, alpha0, alpha1, mid_w0, mid_w1, alpha, mid_w);
-            MGB_DIM_DISPATCH(c.dim, hogwild_epoch, c, w, eptr, e, alpha, mid_w, s);
+            sgd_sched(cc, e, e0, e1, alpha0, alpha1, mid_w0, mid_w1, alpha, mid_w);
+            MGB_DIM_DISPATCH(cc.dim, hogwild_epoch, cc, w, eptr, e, alpha, mid_w, s);
+            MGB_LAUNCH_CHECK();
+        }
+        if (split) {
+            unpack_edges_kernel<<<blocks_for(c.n_edges, kThreads), kThreads, 0, s>>>(cc.eo, c.n_edges, c.eons, c.eonns);
             MGB_LAUNCH_CHECK();
         }
         return;

@@ -4,6 +4,12 @@
 
 namespace mgb {
 
+// An edge's read-only fields, packed for the split form (one 8-byte load per sample)
+struct alignas(8) EdgeRO {
+    int32_t tail;
+    float eps;
+};
+
 // Everything an epoch kernel reads (the reference's Ctx, src/layout.cpp:69-88), as device pointers plus the
 // scalars derived once per call (src/layout.cpp:421-431).
 struct SgdDev {
@@ -20,6 +26,9 @@ struct SgdDev {
     const float* node_b;
     float* adam_m; float* adam_v; int32_t* adam_t; float beta1, beta2;
     uint64_t seed;
+    // the split form's packed copies for one call: (eons, eonns) per edge, and (tail, eps) per edge
+    float2* eo = nullptr;
+    const EdgeRO* te = nullptr;
 };
 
 // launches F<2>, F<3> or the generic F<0> (dims up to kMaxDim) for a layout of `dim` columns
@@ -34,6 +43,7 @@ struct SgdDev {
 struct SgdWork {
     DevBuf cnt, state, delta, eptr, flag;
     DevBuf samp;               // the epoch's sampled set (counter mode fast path)
+    DevBuf pack;               // the split form's packed edge fields
     // owner mode: node rows, chunk bounds, per-edge negatives, per-node stream states, marked chunks, snapshots
     DevBuf o_row, o_own, o_neg, o_state, o_dirty, o_snap, o_snap_m, o_snap_v, o_snap_t;
 };

@@ -52,6 +52,8 @@ def _lib():
         P_, I64 = ctypes.c_void_p, ctypes.c_int64
         lib.mg_knn_search.argtypes = [P_, I64, ctypes.c_int, P_, P_, I64, P_, I64, P_, I64, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, ctypes.c_uint64, ctypes.c_int, P_, P_]
+        lib.mg_transform_schedule.argtypes = [P_, P_, I64, ctypes.c_int, I64, ctypes.c_double, ctypes.c_int, P_, P_,
+                                              P_, ctypes.POINTER(I64)]
         _LIB = lib
     return _LIB
 
@@ -307,14 +309,21 @@ class FittedLayout:
                 raise RuntimeError(_lib().mg_last_error().decode())
             W = vals / torch.clamp(vals.sum(1, keepdim=True), min=1e-12)
             Y_new = torch.einsum("mk,mkd->md", W, self.Yd[ind])
-            # the edge schedule of MAGNET.transform (magnet/__init__.py:907-912), on the host as the reference
-            w = vals.cpu().numpy().ravel().astype(np.float64)
-            freq = D.sampling_frequencies(w, self.samples_per_node * m)
-            keep = freq >= 1.0 / self.epochs
-            ind_h = ind.cpu().numpy().ravel()
-            head = torch.from_numpy((self.n + np.repeat(np.arange(m), self.k)).astype(np.int32)[keep]).to(self.dev)
-            tail = torch.from_numpy(ind_h.astype(np.int32)[keep]).to(self.dev)
-            eps = torch.from_numpy((1.0 / freq[keep]).astype(np.float32)).to(self.dev)
+            # the edge schedule of MAGNET.transform (magnet/__init__.py:907-912), on the device
+            ind = ind.long().contiguous()
+            vals = vals.contiguous()
+            n_e = m * self.k
+            head = torch.empty(n_e, dtype=torch.int32, device=self.dev)
+            tail = torch.empty(n_e, dtype=torch.int32, device=self.dev)
+            eps = torch.empty(n_e, dtype=torch.float32, device=self.dev)
+            kept = ctypes.c_int64(0)
+            rc = _lib().mg_transform_schedule(ctypes.c_void_p(vals.data_ptr()), ctypes.c_void_p(ind.data_ptr()), m,
+                                              self.k, self.n, float(self.samples_per_node), self.epochs,
+                                              ctypes.c_void_p(head.data_ptr()), ctypes.c_void_p(tail.data_ptr()),
+                                              ctypes.c_void_p(eps.data_ptr()), ctypes.byref(kept))
+            if rc != 0:
+                raise RuntimeError(_lib().mg_last_error().decode())
+            head, tail, eps = head[:kept.value], tail[:kept.value], eps[:kept.value]
             Y_all = torch.cat([self.Yd, Y_new.to(torch.float32)]).contiguous()
             eons = eps.clone()
             eonns = (eps / 5.0).contiguous()

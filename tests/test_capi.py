@@ -92,3 +92,18 @@ def test_owner_mode_argument_rules_without_gpu(golden):
     with pytest.raises(RuntimeError, match="owner_chunk_edges"):
         mg.optimize_layout(*args, n_threads=1, parallel=1, owner_chunk_edges=-1, **kw)
     assert np.array_equal(Y, C.owner_state(g, "b1_pairs")[1])
+
+
+def test_transform_schedule_argument_errors_without_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(LIB)
+    lib.mg_last_error.restype = ctypes.c_char_p
+    P, I64 = ctypes.c_void_p, ctypes.c_int64
+    lib.mg_transform_schedule.argtypes = [P, P, I64, ctypes.c_int, I64, ctypes.c_double, ctypes.c_int, P, P, P,
+                                          ctypes.POINTER(I64)]
+    kept = I64(0)
+    rc = lib.mg_transform_schedule(None, None, 4, 3, 10, 5.0, 0, None, None, None, ctypes.byref(kept))
+    assert rc == 1 and b"n_epochs" in lib.mg_last_error()
+    rc = lib.mg_transform_schedule(None, None, 4, 3, 10, 5.0, 100, None, None, None, None)
+    assert rc == 1 and b"n_kept" in lib.mg_last_error()
