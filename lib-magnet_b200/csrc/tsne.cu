@@ -149,6 +149,15 @@ __device__ BBox block_bbox(BBox v) {
     return v;
 }
 
+// the last block of a grid merges the grid's partial boxes, every thread a strided share, then one block reduction
+// (one thread walking them in turn took about 40 us for 592 partials at the loads' latency); the box is exact,
+// whatever the order; the result is in thread 0
+__device__ BBox merge_parts(const BBox* part) {
+    BBox t{INFINITY, INFINITY, -INFINITY, -INFINITY};
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) t = bbox_merge(t, ld_bbox(part, b));
+    return block_bbox(t);
+}
+
 __global__ void bbox_kernel(const float2* __restrict__ Y, int64_t n, BBox* __restrict__ part,
                             unsigned* __restrict__ counter, float* __restrict__ out4) {
     __shared__ int is_last;
@@ -160,10 +169,10 @@ __global__ void bbox_kernel(const float2* __restrict__ Y, int64_t n, BBox* __res
     v = block_bbox(v);
     if (threadIdx.x == 0) { part[blockIdx.x] = v; __threadfence(); is_last = atomicAdd(counter, 1u) == gridDim.x - 1; }
     __syncthreads();
-    if (!is_last || threadIdx.x != 0) return;
+    if (!is_last) return;
     __threadfence();
-    BBox t = ld_bbox(part, 0);
-    for (unsigned b = 1; b < gridDim.x; ++b) t = bbox_merge(t, ld_bbox(part, b));
+    const BBox t = merge_parts(part);
+    if (threadIdx.x != 0) return;
     out4[0] = t.x0; out4[1] = t.y0; out4[2] = t.x1; out4[3] = t.y1;
     *counter = 0u;
 }
@@ -212,10 +221,10 @@ __global__ void __launch_bounds__(kThreads) loop_bbox_kernel(const float2* __res
     v = block_bbox(v);
     if (threadIdx.x == 0) { part[blockIdx.x] = v; __threadfence(); is_last = atomicAdd(&g->counter2, 1u) == gridDim.x - 1; }
     __syncthreads();
-    if (!is_last || threadIdx.x != 0) return;
+    if (!is_last) return;
     __threadfence();
-    BBox t = ld_bbox(part, 0);
-    for (unsigned b = 1; b < gridDim.x; ++b) t = bbox_merge(t, ld_bbox(part, b));
+    const BBox t = merge_parts(part);
+    if (threadIdx.x != 0) return;
     choose_grid(g, t, s, fft_len);
     g->counter2 = 0u;
 }
@@ -338,13 +347,26 @@ __global__ void __launch_bounds__(kThreads) loop_iter_kernel(const float2* __res
         is_last = atomicAdd(&gd->counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!is_last || threadIdx.x != 0) return;
+    if (!is_last) return;
     __threadfence();
+    // the last block sums the partial sums, every thread a strided share, then a fixed-order block reduction (the
+    // same bits from run to run)
     double tx = 0.0, ty = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
         const double2 v = __ldcg(&mpart[b]);
         tx += v.x; ty += v.y;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        tx += __shfl_xor_sync(0xffffffffu, tx, o);
+        ty += __shfl_xor_sync(0xffffffffu, ty, o);
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_double2(tx, ty);
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    tx = 0.0; ty = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tx += red[w].x; ty += red[w].y; }
     gd->mean[0] = (float)(tx / (double)n);
     gd->mean[1] = (float)(ty / (double)n);
     gd->recentre = 1;
