@@ -497,7 +497,40 @@ __device__ __forceinline__ void range_sample(const SgdDev& c, int64_t u, int64_t
 // thread finds its first sample by a binary search of the chunks' prefix sums and a walk of one chunk.
 constexpr int kChunkWords = 64;   // 2048 edges per chunk
 
-__global__ void offsets_kernel(const int32_t* __restrict__ cnt, int64_t n, int64_t* __restrict__ off, int64_t* total);
+// the chunks' exclusive prefix sums and, in cpre[n], the total: one block, each thread a run of consecutive
+// chunks (summed, then a block scan of the run sums, then the run written), so the scan waits on one round of loads
+// instead of one per 1024 chunks
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) chunk_scan_kernel(const int32_t* __restrict__ count, int64_t n,
+                                                                   int64_t* __restrict__ cpre) {
+    __shared__ int64_t wsum[kScanThreads / 32];
+    const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+    const int64_t b = (int64_t)threadIdx.x * per, e = b + per < n ? b + per : n;
+    int64_t run = 0;
+    for (int64_t i = b; i < e; ++i) run += count[i];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int64_t w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    int64_t acc = x - run + (warp > 0 ? wsum[warp - 1] : 0);
+    for (int64_t i = b; i < e; ++i) { cpre[i] = acc; acc += count[i]; }
+    if (threadIdx.x == blockDim.x - 1) cpre[n] = acc;
+}
 
 // the bit set (bit i of bits[i / 32] set when edge i is sampled), one warp ballot per 32 edges and one warp per
 // chunk, and the chunk's count of sampled edges; words past the last edge are written as 0, so every chunk is whole
@@ -628,7 +661,7 @@ void launch_split(const SgdDev& c, int64_t threads, const int64_t* eptr, uint32_
     chunk_bits_kernel<<<blocks_for(n_chunks * 32, kThreads, 8), kThreads, 0, s>>>(c.eo, c.n_edges, (float)epoch,
                                                                                   n_chunks, bits, count);
     MGB_LAUNCH_CHECK();
-    offsets_kernel<<<1, 1024, 0, s>>>(count, n_chunks, cpre, cpre + n_chunks);
+    chunk_scan_kernel<<<1, kScanThreads, 0, s>>>(count, n_chunks, cpre);
     MGB_LAUNCH_CHECK();
     const bool rep1 = FAST && c.rep_b_is_one, b1 = FAST && c.b_is_one;
     auto kernel = rep1 && b1 ? hogwild_split_kernel<D, FAST, true, true>
@@ -636,11 +669,12 @@ void launch_split(const SgdDev& c, int64_t threads, const int64_t* eptr, uint32_
                 : b1         ? hogwild_split_kernel<D, FAST, false, true>
                              : hogwild_split_kernel<D, FAST, false, false>;
     // few threads (small layouts): blocks of fewer threads, so that they spread over every SM
-    int tpb = kThreads;
-    if (threads < (int64_t)kNumSMs * kThreads)
+    int tpb = std::min(kThreads, std::max(32, env_int("MGB_SGD_BLOCK", kThreads) / 32 * 32));
+    if (threads < (int64_t)kNumSMs * tpb)
         tpb = (int)std::min<int64_t>(kThreads, std::max<int64_t>(32, ((threads + kNumSMs - 1) / kNumSMs + 31) / 32 * 32));
     int64_t blocks = std::max<int64_t>(1, (threads + tpb - 1) / tpb);
     if (tpb == kThreads) blocks = std::min<int64_t>(blocks, resident_blocks(kernel));
+    else blocks = std::min<int64_t>(blocks, (int64_t)resident_blocks(kernel) * (kThreads / tpb));
     kernel<<<(int)blocks, tpb, 0, s>>>(c, eptr, bits, cpre, n_chunks, epoch, alpha, mid_w);
 }
 
