@@ -208,6 +208,18 @@ int mg_layout_schedule(const mg_layout_args* a, int epoch, uint8_t* sampled, int
  * log2(n_neighbors) * bandwidth in n_iter steps at most. */
 int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter, float* out);
 
+/* chebyshev_eigenvectors (src/spectral.cpp:141-241, bound at src/bindings.cpp; called by magnet/spectral.py:8-46,
+ * the spectral initialisation): the Chebyshev-filtered subspace iteration with Rayleigh-Ritz for the leading
+ * non-trivial eigenvectors of the lazy normalised adjacency (I + D^-1/2 A D^-1/2) / 2 of the graph (indptr,
+ * indices, data; n nodes, nnz entries), the trivial eigenvector deflated per connected component (component
+ * labels >= 0). X (n, p) row major: the start block in, the Ritz vectors out, columns by descending Ritz value.
+ * inv_sqrt_deg: 1 / sqrt(degree) per node (0 where the degree is 0). 1 <= n_wanted < p <= 8 (larger p returns
+ * MG_ERR_NOT_SUPPORTED), degree >= 2, max_iter >= 0, the reference's stopping rule with tol. FP64 on the device;
+ * host or device arrays. Synchronises the stream. */
+int mg_chebyshev_eigenvectors(const int32_t* indptr, const int32_t* indices, const float* data, int64_t n,
+                              int64_t nnz, float* X, int p, const float* inv_sqrt_deg, const int32_t* component,
+                              int n_wanted, int degree, int max_iter, float tol);
+
 /* The edge schedule of MAGNET.transform (magnet/__init__.py:907-912, with _sampling_frequencies of
  * magnet/__init__.py:51-66), on the device: w (m, k) memberships of m new rows and ind (m, k) their neighbours
  * among n_train fixed rows -> the kept edges in row order, head[e] = n_train + row, tail[e] = ind, eps[e] = 1 / freq,

@@ -2,8 +2,9 @@
 
 Put the directory holding this package ahead of the reference's extension on sys.path; the reference's Python
 package (`magnet`) then runs its layout pass on the B200: optimize_layout, FFTConv2D, tsne_attraction, tsne_step,
-tsne_update, bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense and knn_search come from the device library. The
-host-side kernels that stay on the reference's code (nn_descent, the sparse-data searches, spectral init, louvain)
+tsne_update, bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense, knn_search and chebyshev_eigenvectors (blocks of
+up to 8 columns) come from the device library. The host-side kernels that stay on the reference's code
+(nn_descent, the sparse-data searches, subspace_iteration, louvain)
 are forwarded to the reference's own compiled module, found through the MAGNET_HOST_MODULE environment variable
 (path to the reference's `_magnet*.so`); without it they raise ImportError when used, as a missing `_magnet` would.
 """
@@ -14,7 +15,8 @@ import sys as _sys
 from magnet_b200._native import (FFTConv2D, optimize_layout, tsne_attraction, tsne_step, tsne_update,  # noqa: F401
                                  bbox_2d, mid_spring, smooth_knn, mid_near_pairs_dense, knn_search)
 
-_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search_sparse", "mid_near_pairs_sparse", "chebyshev_eigenvectors", "subspace_iteration", "louvain", "interp_scatter",
+_HOST_NAMES = ("nn_descent", "nn_descent_sparse", "knn_search_sparse", "mid_near_pairs_sparse", "subspace_iteration",
+               "louvain", "interp_scatter",
                "interp_gather", "scatter_padded_2d", "spectral_products", "gather_forces_2d", "umap_attraction")
 
 
@@ -36,6 +38,21 @@ def _load_host():
 
 
 _host = _load_host()
+
+
+def chebyshev_eigenvectors(indptr, indices, data, X, inv_sqrt_deg, component, n_wanted, degree, max_iter, tol,
+                           n_threads=-1):
+    """src/spectral.cpp:141-241 on the device for blocks of up to 8 columns (magnet/spectral.py asks for
+    n_components + max(2, n_components)); wider blocks go to the reference's host module"""
+    from magnet_b200 import _native
+    if getattr(X, "shape", (0, 0))[1] <= 8:
+        return _native.chebyshev_eigenvectors(indptr, indices, data, X, inv_sqrt_deg, component, n_wanted, degree,
+                                              max_iter, tol, n_threads)
+    if _host is None:
+        raise ImportError("_magnet.chebyshev_eigenvectors with more than 8 columns runs on the reference's host "
+                          "module; set MAGNET_HOST_MODULE to its path")
+    return _host.chebyshev_eigenvectors(indptr, indices, data, X, inv_sqrt_deg, component, n_wanted, degree,
+                                        max_iter, tol, n_threads)
 
 
 def __getattr__(name):

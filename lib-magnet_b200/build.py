@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 
 # per-file flags: owner mode and the graph passes round every product and sum on their own, as the reference's
 # plain x86-64 build and numpy do
-FILE_FLAGS = {"owner.cu": ["-fmad=false"], "graph.cu": ["-fmad=false"]}
+FILE_FLAGS = {"owner.cu": ["-fmad=false"], "graph.cu": ["-fmad=false"], "spectral.cu": ["-fmad=false"]}
 
 
 def _newer(target, deps):

@@ -6,6 +6,7 @@
 #include "tsne.cuh"
 #include "sgd.cuh"
 #include "graph.cuh"
+#include "spectral.cuh"
 #include <string>
 #include <vector>
 #include <memory>
@@ -661,6 +662,11 @@ GraphWork& graph_work() {
     if (!g_graph_work) g_graph_work.reset(new GraphWork());
     return *g_graph_work;
 }
+thread_local std::unique_ptr<SpecWork> g_spec_work;
+SpecWork& spec_work() {
+    if (!g_spec_work) g_spec_work.reset(new SpecWork());
+    return *g_spec_work;
+}
 }  // namespace
 
 extern "C" int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbors, float bandwidth, int n_iter,
@@ -676,6 +682,48 @@ extern "C" int mg_smooth_knn(const float* dist, int64_t n, int k, int n_neighbor
         smooth_knn_dev(d, n, k, target, n_iter, o, graph_work(), s);
         back(out, o, n * k, s);
         if (any_host({dist, out})) MGB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" int mg_chebyshev_eigenvectors(const int32_t* indptr, const int32_t* indices, const float* data,
+                                         int64_t n, int64_t nnz, float* X, int p, const float* inv_sqrt_deg,
+                                         const int32_t* component, int n_wanted, int degree, int max_iter,
+                                         float tol) {
+    return guard([&] {
+        // the argument rules of src/spectral.cpp:146-157
+        require(X && n >= 1 && p >= 1, "X must be 2-d");
+        require(n_wanted >= 1 && n_wanted < p, "X needs at least n_wanted + 1 columns");
+        require(degree >= 2 && max_iter >= 0, "degree must be >= 2");
+        require(indptr && (nnz == 0 || (indices && data)), "the graph must be a CSR matrix");
+        require(inv_sqrt_deg, "inv_sqrt_deg must have n entries");
+        require(component, "component must have n entries");
+        require(n <= INT32_MAX, "n must fit 32-bit indices");
+        if (p > kSpecMaxCols) throw Error(MG_ERR_NOT_SUPPORTED, "the device solver takes at most 8 columns");
+        validate_csr_host(indptr, indices, nnz, n, -1, "chebyshev_eigenvectors");
+        // the component labels on the host: their count sizes the per-component sums
+        std::vector<int32_t> comp_h;
+        const int32_t* ch = component;
+        if (is_device_ptr(component)) {
+            comp_h.resize((size_t)n);
+            MGB_CUDA(cudaMemcpy(comp_h.data(), component, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost));
+            ch = comp_h.data();
+        }
+        int32_t n_comp = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            require(ch[i] >= 0, "component labels must be >= 0");
+            n_comp = std::max(n_comp, ch[i] + 1);
+        }
+        cudaStream_t s = current_stream();
+        const int32_t* ip = in_dev(indptr, n + 1, 0, s);
+        const int32_t* ix = in_dev(indices, nnz, 1, s);
+        const float* pd = in_dev(data, nnz, 2, s);
+        const float* sd = in_dev(inv_sqrt_deg, n, 3, s);
+        const int32_t* cd = in_dev(component, n, 4, s);
+        float* xd = in_dev(X, n * p, 5, s);
+        chebyshev_eigenvectors_dev(ip, ix, pd, n, sd, cd, n_comp, xd, p, n_wanted, degree, max_iter, (double)tol,
+                                   spec_work(), s);
+        back(X, xd, n * p, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -276,6 +276,29 @@ py::tuple knn_search(py::object X, py::object gptr, py::object gidx, py::object 
     return py::make_tuple(oi, od);
 }
 
+// chebyshev_eigenvectors (src/spectral.cpp:141-241) on the device; X is updated in place and returned, as the
+// reference returns its X argument
+py::object chebyshev_eigenvectors(py::object indptr, py::object indices, py::object data, py::object X,
+                                  py::object inv_sqrt_deg, py::object component, int n_wanted, int degree,
+                                  int max_iter, float tol, int n_threads) {
+    (void)n_threads;   // the device solver does not take a host thread count
+    auto ip = view<int32_t>(indptr), ix = view<int32_t>(indices), cp = view<int32_t>(component);
+    auto pd = view<float>(data), sd = view<float>(inv_sqrt_deg);
+    auto x = view<float>(X);
+    if (x.ndim() != 2) throw std::runtime_error("X must be 2-d");
+    const int64_t n = x.dim(0);
+    if (ip.size() != n + 1) throw std::runtime_error("indptr must have n + 1 entries");
+    if (ix.size() != pd.size()) throw std::runtime_error("indices and data must have the same length");
+    if (sd.ndim() != 1 || sd.dim(0) != n) throw std::runtime_error("inv_sqrt_deg must have n entries");
+    if (cp.ndim() != 1 || cp.dim(0) != n) throw std::runtime_error("component must have n entries");
+    {
+        py::gil_scoped_release rel;
+        check(mg_chebyshev_eigenvectors(ip.ptr, ix.ptr, pd.ptr, n, ix.size(), x.ptr, (int)x.dim(1), sd.ptr, cp.ptr,
+                                        n_wanted, degree, max_iter, tol));
+    }
+    return x.keep;
+}
+
 // the fuzzy union of magnet/knn.py:221-230 on the device: (indptr, indices, data) of the n x n CSR
 py::tuple fuzzy_union(py::object ind, py::object vals, int64_t n, double set_op_mix_ratio) {
     auto id = view<int32_t>(ind);
@@ -398,6 +421,11 @@ PYBIND11_MODULE(_native, m) {
     m.def("knn_search", &knn_search, "Beam search of queries over a neighbour graph (dense data, device)",
           py::arg("X"), py::arg("gptr"), py::arg("gidx"), py::arg("landmarks"), py::arg("Q"), py::arg("k"),
           py::arg("ef") = 64, py::arg("n_entry") = 10, py::arg("seed") = 0, py::arg("n_threads") = -1);
+    m.def("chebyshev_eigenvectors", &chebyshev_eigenvectors,
+          "Chebyshev-filtered subspace iteration for the leading non-trivial eigenvectors (device)",
+          py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("X"), py::arg("inv_sqrt_deg"),
+          py::arg("component"), py::arg("n_wanted"), py::arg("degree"), py::arg("max_iter"), py::arg("tol"),
+          py::arg("n_threads") = -1);
     m.def("fuzzy_union", &fuzzy_union, "fuzzy union A + A^T - A o A^T of kNN memberships (device): (indptr, indices, data)",
           py::arg("ind"), py::arg("vals"), py::arg("n") = -1, py::arg("set_op_mix_ratio") = 1.0);
     m.def("tsne_attraction", [](py::object indptr, py::object indices, py::object data, py::object Y, float dof, int) {

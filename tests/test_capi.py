@@ -107,3 +107,19 @@ def test_transform_schedule_argument_errors_without_gpu():
     assert rc == 1 and b"n_epochs" in lib.mg_last_error()
     rc = lib.mg_transform_schedule(None, None, 4, 3, 10, 5.0, 100, None, None, None, None)
     assert rc == 1 and b"n_kept" in lib.mg_last_error()
+
+
+def test_chebyshev_argument_errors_without_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(LIB)
+    lib.mg_last_error.restype = ctypes.c_char_p
+    P, I64 = ctypes.c_void_p, ctypes.c_int64
+    lib.mg_chebyshev_eigenvectors.argtypes = [P, P, P, I64, I64, P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_float]
+    import numpy as np
+    X = np.zeros((4, 3), np.float32)
+    rc = lib.mg_chebyshev_eigenvectors(None, None, None, 4, 0, X.ctypes.data, 3, None, None, 3, 30, 5, 0.05)
+    assert rc == 1 and b"n_wanted + 1 columns" in lib.mg_last_error()
+    rc = lib.mg_chebyshev_eigenvectors(None, None, None, 4, 0, X.ctypes.data, 3, None, None, 2, 1, 5, 0.05)
+    assert rc == 1 and b"degree must be >= 2" in lib.mg_last_error()

@@ -5,12 +5,13 @@ MAGNET.fit_transform with loss "umap", "tsne" and "hybrid", and MAGNET.transform
 
 The calls were recorded by running the reference's estimator unchanged on top of a recording stand-in for its
 `_magnet` (tests/golden/make_dropin_golden.py): its Python package cannot travel to the GPU machine, so the
-estimator itself cannot run there. The layout-pass entry points run on the device; the host-side ones (kNN,
-spectral init, mid-near partners) are forwarded to the reference's compiled module (oracle/_ref) through
-MAGNET_HOST_MODULE, as the drop-in is meant to be installed.
+estimator itself cannot run there. The layout-pass entry points, the mid-near partners, the query search and the
+spectral solver run on the device; NN-descent is forwarded to the reference's compiled module (oracle/_ref)
+through MAGNET_HOST_MODULE, as the drop-in is meant to be installed.
 
 Bounds per entry point (the same as the entry points' own tests): bbox_2d exact; tsne_attraction, tsne_step,
 tsne_update, mid_spring and smooth_knn within 1e-5 relative; FFTConv2D.compute's sumQ and F within 1e-4 relative;
+chebyshev_eigenvectors' leading Ritz vectors spanning the reference's subspace (largest principal-angle sine 1e-3);
 optimize_layout's schedule state (epoch_of_next_sample, epoch_of_next_negative_sample) bit-exact, its layout (the
 device's own random streams) finite and moved by as much as the reference's within a factor of 2.
 """
@@ -60,6 +61,14 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
+def subspace_sine(A, B):
+    """the largest sine of the principal angles between the column spans of A and B"""
+    qa, _ = np.linalg.qr(A)
+    qb, _ = np.linalg.qr(B)
+    cos = np.clip(np.linalg.svd(qa.T @ qb, compute_uv=False), 0.0, 1.0)
+    return float(np.sqrt(max(0.0, 1.0 - cos.min() ** 2)))
+
+
 def check_call(g, c, args, out):
     name = c["name"]
     ret = decode(g, c["ret"])
@@ -84,8 +93,14 @@ def check_call(g, c, args, out):
         return args[0]
     elif name in ("mid_near_pairs_dense", "knn_search"):
         o, r = (out, ret) if name == "mid_near_pairs_dense" else (out[0], ret[0])
-        assert np.array_equal(np.asarray(o), np.asarray(r))   # forwarded to the reference's module
-    elif name in ("nn_descent", "chebyshev_eigenvectors"):
+        assert np.array_equal(np.asarray(o), np.asarray(r))   # the device reproduces the reference's streams
+    elif name == "chebyshev_eigenvectors":
+        # on the device now: the leading n_wanted Ritz vectors span the reference's subspace
+        o, r = np.asarray(out, np.float64), np.asarray(ret, np.float64)
+        nw = int(args[6])
+        assert o.shape == r.shape and np.isfinite(o).all()
+        assert subspace_sine(o[:, :nw], r[:, :nw]) < 1e-3, subspace_sine(o[:, :nw], r[:, :nw])
+    elif name == "nn_descent":
         o = out[0] if isinstance(out, tuple) else out
         r = ret[0] if isinstance(ret, tuple) else ret
         assert np.asarray(o).shape == np.asarray(r).shape     # forwarded; multithreaded on the host

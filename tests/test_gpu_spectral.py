@@ -1,0 +1,124 @@
+"""The spectral initialisation's solver on the device (chebyshev_eigenvectors, src/spectral.cpp:141-241, as
+magnet/spectral.py:8-46 calls it) against the reference's own compiled solver on the same graph and start block:
+the leading n_wanted Ritz vectors span the same subspace (largest principal-angle sine below 1e-3), their Ritz
+values agree to 1e-6, and the layout that spectral_init makes of them (the vectors scaled by 1 / sqrt(degree))
+matches up to the orientation of each axis. Cases: the 10,000-point graph of the loss="umap" configuration (the
+reference's own fuzzy graph), a graph of three connected components plus isolated nodes (per-component
+deflation, zero degrees), and a 3-d layout (six columns)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+from scipy.sparse.csgraph import connected_components
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+
+pytestmark = pytest.mark.gpu
+
+
+def subspace_sine(A, B):
+    qa, _ = np.linalg.qr(np.asarray(A, np.float64))
+    qb, _ = np.linalg.qr(np.asarray(B, np.float64))
+    cos = np.clip(np.linalg.svd(qa.T @ qb, compute_uv=False), 0.0, 1.0)
+    return float(np.sqrt(max(0.0, 1.0 - cos.min() ** 2)))
+
+
+def ritz_values(P, sd, X):
+    """the Rayleigh quotients of the columns of X under M = (I + D^-1/2 P D^-1/2) / 2"""
+    D = sp.diags(sd.astype(np.float64))
+    M = 0.5 * (sp.identity(P.shape[0]) + D @ P.astype(np.float64) @ D)
+    X = np.asarray(X, np.float64)
+    return np.einsum("ij,ij->j", X, M @ X) / np.einsum("ij,ij->j", X, X)
+
+
+def inputs(P, n_components, seed=0):
+    """the arguments spectral_init builds (magnet/spectral.py:14-31)"""
+    P = sp.csr_matrix(P, dtype=np.float32)
+    n = P.shape[0]
+    deg = np.asarray(P.sum(1)).ravel().astype(np.float64)
+    sd = np.where(deg > 0, 1.0 / np.sqrt(np.maximum(deg, 1e-12)), 0.0).astype(np.float32)
+    _, comp = connected_components(P, directed=False)
+    extra = max(2, n_components)
+    X = np.random.default_rng(seed).standard_normal((n, n_components + extra)).astype(np.float32)
+    degree = 30
+    max_iter = int(max(3, min(25, int(3e9 / max(1, P.nnz * (n_components + extra) * degree)))))
+    return (P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data.astype(np.float32), X, sd,
+            comp.astype(np.int32), n_components, degree, max_iter, 0.05)
+
+
+def compare(mg, ref, P, n_components, seed=0):
+    from magnet_b200 import _native as N
+    a = inputs(P, n_components, seed)
+    Xd = N.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1)
+    Xr = np.asarray(ref.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1))
+    nw = n_components
+    s = subspace_sine(Xd[:, :nw], Xr[:, :nw])
+    vd, vr = ritz_values(sp.csr_matrix(P), a[4], Xd[:, :nw]), ritz_values(sp.csr_matrix(P), a[4], Xr[:, :nw])
+    # the layout spectral_init makes: the vectors scaled by 1 / sqrt(degree), each axis up to its sign
+    Ld, Lr = Xd[:, :nw] * a[4][:, None], Xr[:, :nw] * a[4][:, None]
+    axes = [min(np.linalg.norm(Ld[:, c] - Lr[:, c]), np.linalg.norm(Ld[:, c] + Lr[:, c])) /
+            max(np.linalg.norm(Lr[:, c]), 1e-30) for c in range(nw)]
+    print("n=%d p=%d: principal-angle sine %.2e, Ritz values %s / %s, axis errors %s"
+          % (P.shape[0], a[3].shape[1], s, np.round(vd, 7), np.round(vr, 7), np.round(axes, 6)))
+    assert np.isfinite(Xd).all()
+    assert s < 1e-3
+    assert np.allclose(vd, vr, rtol=0, atol=1e-6)
+    return axes
+
+
+def test_umap_configuration_graph(mg, ref, golden):
+    if ref is None:
+        pytest.skip("reference module not built")
+    g = golden("layout_config1.npz")
+    P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(len(g["indptr"]) - 1,) * 2)
+    axes = compare(mg, ref, P, 2)
+    assert max(axes) < 1e-2
+
+
+def three_components(seed=4):
+    rng = np.random.default_rng(seed)
+    blocks = []
+    for size in (700, 400, 250):
+        A = sp.random(size, size, density=12.0 / size, random_state=rng, dtype=np.float32)
+        A = A + A.T + sp.diags(np.ones(size - 1, np.float32), 1) + sp.diags(np.ones(size - 1, np.float32), -1)
+        blocks.append(A)
+    blocks.append(sp.csr_matrix((5, 5), dtype=np.float32))   # five isolated nodes
+    P = sp.block_diag(blocks, format="csr").astype(np.float32)
+    P.data = np.abs(P.data) + 0.05
+    return P
+
+
+def test_components_and_isolated_nodes(mg, ref):
+    if ref is None:
+        pytest.skip("reference module not built")
+    compare(mg, ref, three_components(), 2, seed=1)
+
+
+def test_three_dimensions(mg, ref, golden):
+    if ref is None:
+        pytest.skip("reference module not built")
+    g = golden("layout_config1.npz")
+    P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(len(g["indptr"]) - 1,) * 2)
+    compare(mg, ref, P, 3, seed=2)
+
+
+def test_device_arrays_in_place(mg):
+    import torch
+    from magnet_b200 import _native as N
+    a = inputs(three_components(), 2, seed=3)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    Xd = t(a[3])
+    out = N.chebyshev_eigenvectors(t(a[0]), t(a[1]), t(a[2]), Xd, t(a[4]), t(a[5]), *a[6:], -1)
+    assert out is Xd or out.data_ptr() == Xd.data_ptr()
+    Xh = N.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1)
+    assert subspace_sine(Xd.cpu().numpy()[:, :2], Xh[:, :2]) < 1e-6
+
+
+def test_wide_blocks_rejected(mg):
+    from magnet_b200 import _native as N
+    a = list(inputs(three_components(), 2))
+    a[3] = np.zeros((a[3].shape[0], 9), np.float32)
+    with pytest.raises(RuntimeError, match="at most 8 columns"):
+        N.chebyshev_eigenvectors(*a, -1)
