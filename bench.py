@@ -885,6 +885,72 @@ def fft_grid_bench(n_boxes, steps, warmup, n=300_000, seed=0):
 
 
 # ----------------------------------------------------------------------------------------------- fuzzy graph
+def spectral_inputs(P, n_components=2, seed=0):
+    """the arguments magnet/spectral.py:14-31 builds for chebyshev_eigenvectors"""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import connected_components
+    P = sp.csr_matrix(P, dtype=np.float32)
+    deg = np.asarray(P.sum(1)).ravel().astype(np.float64)
+    sd = np.where(deg > 0, 1.0 / np.sqrt(np.maximum(deg, 1e-12)), 0.0).astype(np.float32)
+    _, comp = connected_components(P, directed=False)
+    extra = max(2, n_components)
+    X = np.random.default_rng(seed).standard_normal((P.shape[0], n_components + extra)).astype(np.float32)
+    degree = 30
+    max_iter = int(max(3, min(25, int(3e9 / max(1, P.nnz * (n_components + extra) * degree)))))
+    return (P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data.astype(np.float32), X, sd,
+            comp.astype(np.int32), n_components, degree, max_iter, 0.05)
+
+
+def spectral_bench(n, steps, warmup, cpu_baseline=True):
+    """The spectral initialisation's solver (chebyshev_eigenvectors, src/spectral.cpp:141-241, with the arguments
+    of magnet/spectral.py) on the workload's fuzzy graph: the device solver on device-resident arrays (CUDA
+    events), through host arrays (end to end), and the reference's compiled solver on all host threads, with the
+    largest principal-angle sine between the two results' leading vectors. One JSON line."""
+    import torch
+    from magnet_b200 import _native as N
+    w = make_workload(n)
+    a = spectral_inputs(w["P"])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    ad = [t(a[0]), t(a[1]), t(a[2]), None, t(a[4]), t(a[5])]
+    X0 = t(a[3])
+    times, e2e = [], []
+    Xd = None
+    for i in range(warmup + steps):
+        Xd = X0.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        N.chebyshev_eigenvectors(ad[0], ad[1], ad[2], Xd, ad[4], ad[5], *a[6:], -1)
+        e1.record()
+        torch.cuda.synchronize()
+        h0 = time.perf_counter()
+        N.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1)
+        h1 = time.perf_counter()
+        if i >= warmup:
+            times.append(e0.elapsed_time(e1) / 1000)
+            e2e.append(h1 - h0)
+    out = {"metric": "spectral init solver s (chebyshev_eigenvectors, %d x %d block)" % a[3].shape, "unit": "s",
+           "higher_is_better": False, "steps": steps, "warmup": warmup, "dtype": "f64",
+           "config": {"workload": "the fuzzy graph of the %d-point hybrid workload" % n, "nnz": int(w["P"].nnz),
+                      "degree": a[7], "max_iter": a[8]},
+           "value": round(statistics.median(times), 5), "e2e": {"value": round(statistics.median(e2e), 5), "unit": "s"}}
+    if cpu_baseline:
+        from oracle import oracle as O
+        R = O.reference()
+        if R is not None:
+            h0 = time.perf_counter()
+            Xr = np.asarray(R.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1))
+            ref_s = time.perf_counter() - h0
+            qa, _ = np.linalg.qr(Xd.cpu().numpy()[:, :2].astype(np.float64))
+            qb, _ = np.linalg.qr(Xr[:, :2].astype(np.float64))
+            cos = np.clip(np.linalg.svd(qa.T @ qb, compute_uv=False), 0.0, 1.0)
+            out["cpu_baseline"] = {"value": round(ref_s, 3), "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+                                   "sample": "one whole call of the reference's compiled solver on the same inputs"}
+            out["subspace_sine"] = float(np.sqrt(max(0.0, 1.0 - cos.min() ** 2)))
+    print(json.dumps(out))
+
+
 def graph_bench(n, steps, warmup, cpu_baseline=True):
     """The fuzzy neighbour graph of the workload (smooth_knn + fuzzy union, magnet/knn.py:215-230) on the device:
     device-resident passes timed with CUDA events through the C ABI, the package's fuzzy_graph on host arrays
@@ -1180,6 +1246,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graph", action="store_true", help="time the fuzzy neighbour graph instead of the layout")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--spectral", action="store_true", help="time the spectral initialisation's solver")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--fft-grid", type=int, default=0, help="time the FFT pass alone at this many boxes per side")
     ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4],
@@ -1204,6 +1271,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         graph_bench(args.n, args.steps, args.warmup, not args.no_cpu_baseline)
+        return
+    if args.spectral:
+        import torch
+        torch.cuda.set_device(0)
+        spectral_bench(args.n, args.steps, args.warmup, not args.no_cpu_baseline)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
