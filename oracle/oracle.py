@@ -12,7 +12,8 @@ as the checker or as the timed CPU baseline. It gives:
   (magnet/__init__.py:51-66, 727-737) and ``optimize_sgd`` (MAGNET._optimize, magnet/__init__.py:751-839,
   integer-epoch path);
 * ``fft_repulsion_fp64``: the FFT-interpolated repulsion with the reference's spread/gather and an FP64
-  convolution, and ``exact_repulsion``: the FP64 all-pairs sums.
+  convolution, and ``exact_repulsion``: the FP64 all-pairs sums;
+* ``chebyshev_eigenvectors``: a numpy restatement of the spectral init's solver (src/spectral.cpp:141-241).
 """
 import ctypes
 import importlib.util
@@ -607,3 +608,94 @@ def optimize_tsne(P, Y, n_iter=750, early_iter=250, early_exaggeration=12.0, exa
     run = TsneRun(P, Y, n_iter, early_iter, early_exaggeration, exaggeration, learning_rate, momentum, n_interp,
                   box_width, n_threads, dof, backend, callback)
     return run.advance(n_iter)
+
+
+# ---------------------------------------------------------------------------------------------- spectral init
+def _jacobi_eigen(H):
+    """cyclic Jacobi rotations on a small symmetric matrix (Golub and Van Loan, section 8.5), as
+    src/spectral.cpp:87-123 runs them: eigenvalues descending, eigenvectors as columns"""
+    A = np.array(H, dtype=np.float64)
+    p = A.shape[0]
+    V = np.eye(p)
+    for _ in range(100):
+        if sum(A[i, j] ** 2 for i in range(p) for j in range(i + 1, p)) < 1e-22:
+            break
+        for i in range(p):
+            for j in range(i + 1, p):
+                aij = A[i, j]
+                if abs(aij) < 1e-300:
+                    continue
+                th = (A[j, j] - A[i, i]) / (2.0 * aij)
+                t = (1.0 if th >= 0 else -1.0) / (abs(th) + np.sqrt(th * th + 1.0))
+                c = 1.0 / np.sqrt(t * t + 1.0)
+                s = t * c
+                for M in (A, V):
+                    x, y = M[:, i].copy(), M[:, j].copy()
+                    M[:, i], M[:, j] = c * x - s * y, s * x + c * y
+                x, y = A[i, :].copy(), A[j, :].copy()
+                A[i, :], A[j, :] = c * x - s * y, s * x + c * y
+    d = np.diag(A).copy()
+    order = sorted(range(p), key=lambda k: -d[k])
+    return d[order], V[:, order]
+
+
+def chebyshev_eigenvectors(indptr, indices, data, X, inv_sqrt_deg, component, n_wanted, degree, max_iter, tol):
+    """src/spectral.cpp:141-241 in numpy (FP64): the Chebyshev-filtered subspace iteration with Rayleigh-Ritz for
+    the leading non-trivial eigenvectors of (I + D^-1/2 A D^-1/2) / 2, the trivial eigenvector deflated per
+    connected component, two passes of modified Gram-Schmidt; returns the float32 block"""
+    import scipy.sparse as sp
+    n, p = X.shape
+    A = sp.csr_matrix((np.asarray(data, np.float64), indices, indptr), shape=(n, n))
+    sd = np.asarray(inv_sqrt_deg, np.float64)
+    comp = np.asarray(component, np.int64)
+    t = np.where(sd > 0, 1.0 / np.where(sd > 0, sd, 1.0), 0.0)
+    nc = int(comp.max()) + 1
+    tn = np.bincount(comp, weights=t * t, minlength=nc)
+
+    def M(Y):
+        return 0.5 * (Y + sd[:, None] * (A @ (sd[:, None] * Y)))
+
+    def deflate(Y):
+        pr = np.stack([np.bincount(comp, weights=t * Y[:, k], minlength=nc) for k in range(p)], 1)
+        pr = np.where(tn[:, None] > 0, pr / np.where(tn[:, None] > 0, tn[:, None], 1.0), 0.0)
+        return Y - t[:, None] * pr[comp]
+
+    def orthonormalize(Y):
+        for _ in range(2):
+            for k in range(p):
+                for j in range(k):
+                    Y[:, k] -= (Y[:, k] @ Y[:, j]) * Y[:, j]
+                nrm = Y[:, k] @ Y[:, k]
+                Y[:, k] *= 1.0 / np.sqrt(nrm) if nrm > 1e-300 else 0.0
+        return Y
+
+    def rayleigh_ritz(X):
+        Z = deflate(M(X))
+        H = X.T @ Z
+        H = np.triu(H) + np.triu(H, 1).T
+        theta, V = _jacobi_eigen(H)
+        X, Z = X @ V, Z @ V
+        return X, Z, theta, max(np.linalg.norm(Z[:, c] - theta[c] * X[:, c]) for c in range(n_wanted))
+
+    X = orthonormalize(deflate(np.asarray(X, np.float64)))
+    X, Z, theta, res = rayleigh_ritz(X)
+    prev = -1.0
+    for _ in range(max_iter):
+        gap = max(theta[n_wanted - 1] - theta[n_wanted], 1e-3)
+        total = theta[:n_wanted].sum()
+        if res < tol * gap or res < 1e-9 or (prev >= 0 and abs(total - prev) < 1e-9 * n_wanted):
+            break
+        prev = total
+        alpha = max(min(theta[p - 1], theta[n_wanted - 1] - 0.5 * gap), 1e-3)
+        a0 = min(1.0, theta[0] + 1e-9)
+        e = cc = 0.5 * alpha
+        s1 = e / (a0 - cc)
+        sigma = s1
+        Y = (deflate(M(X)) - cc * X) * (s1 / e)
+        for _ in range(2, degree + 1):
+            sn = 1.0 / (2.0 / s1 - sigma)
+            Yn = (deflate(M(Y)) - cc * Y) * (2.0 * sn / e) - sigma * sn * X
+            X, Y, sigma = Y, Yn, sn
+        X = orthonormalize(deflate(Y.copy()))
+        X, Z, theta, res = rayleigh_ritz(X)
+    return X.astype(np.float32)

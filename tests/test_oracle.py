@@ -290,3 +290,25 @@ def test_mid_near_pairs_oracle_matches_reference(ref, n, d, nt, seed):
     rng = np.random.default_rng(n + d)
     X = rng.normal(0, 3, (n, d)).astype(np.float32)
     assert np.array_equal(np.asarray(ref.mid_near_pairs_dense(X, 5, 6, seed, nt)), O.mid_near_pairs(X, 5, 6, seed, nt))
+
+
+@pytest.mark.parametrize("case", ["umap10k", "components"])
+def test_spectral_oracle_matches_reference(ref, case):
+    """the numpy restatement of chebyshev_eigenvectors against the reference's compiled solver: the same Ritz
+    vectors, column by column with the same signs"""
+    if ref is None:
+        pytest.skip("reference module not built")
+    import os
+    import scipy.sparse as sp
+    from spectral_cases import inputs, three_components
+    if case == "umap10k":
+        g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "layout_config1.npz"))
+        P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(len(g["indptr"]) - 1,) * 2)
+    else:
+        P = three_components()
+    a = inputs(P, 2, seed=0)
+    Xo = O.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:])
+    Xr = np.asarray(ref.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1))
+    for c in range(Xo.shape[1]):
+        cos = float(Xo[:, c].astype(np.float64) @ Xr[:, c]) / (np.linalg.norm(Xo[:, c]) * np.linalg.norm(Xr[:, c]))
+        assert cos > 1 - 1e-6, (c, cos)
