@@ -18,8 +18,12 @@ namespace {
 
 constexpr int kSpecThreads = 256;
 
+// blocks of the reductions (their partials go to the host) and of the row-parallel kernels (one row per thread)
 int spec_blocks(int64_t rows) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((rows + kSpecThreads - 1) / kSpecThreads, 4 * kNumSMs));
+}
+int row_blocks(int64_t rows) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((rows + kSpecThreads - 1) / kSpecThreads, 64 * kNumSMs));
 }
 
 // the weight of node i on the trivial eigenvector: 1 / sd_i (0 for isolated nodes)
@@ -247,19 +251,19 @@ __global__ void narrow_kernel(const double* __restrict__ in, float* __restrict__
 template <int P>
 struct Solver {
     const int32_t* indptr; const int32_t* indices; const float* data; const float* sd; const int32_t* comp;
-    int64_t n; int n_comp; int blocks; cudaStream_t s;
+    int64_t n; int n_comp; int blocks; int rblocks; cudaStream_t s;
     double* proj; const double* tnorm; double* part;
     std::vector<double> host_part;
 
     void spmm(const double* in, double* out) {
-        spmm_kernel<P><<<blocks, kSpecThreads, 0, s>>>(indptr, indices, data, sd, n, in, out);
+        spmm_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(indptr, indices, data, sd, n, in, out);
         MGB_LAUNCH_CHECK();
     }
     void deflate(double* X) {
         MGB_CUDA(cudaMemsetAsync(proj, 0, sizeof(double) * (size_t)n_comp * P, s));
-        component_sum_kernel<P><<<blocks, kSpecThreads, 0, s>>>(sd, comp, n, X, false, proj);
+        component_sum_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(sd, comp, n, X, false, proj);
         MGB_LAUNCH_CHECK();
-        deflate_apply_kernel<P><<<blocks, kSpecThreads, 0, s>>>(sd, comp, n, proj, tnorm, X);
+        deflate_apply_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(sd, comp, n, proj, tnorm, X);
         MGB_LAUNCH_CHECK();
     }
     // the p x p matrix A^T B, its block partials added on the host in block order (the same bits every call)
@@ -284,13 +288,13 @@ struct Solver {
                 if (k > 0) {
                     const std::vector<double> G = gram(X, X);
                     for (int j = 0; j < k; ++j) c.v[j] = G[(size_t)k * P + j];
-                    column_update_kernel<P><<<blocks, kSpecThreads, 0, s>>>(X, n, k, c, 1.0);
+                    column_update_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(X, n, k, c, 1.0);
                     MGB_LAUNCH_CHECK();
                 }
                 const std::vector<double> G = gram(X, X);
                 const double nrm = G[(size_t)k * P + k];
                 const double inv = nrm > 1e-300 ? 1.0 / std::sqrt(nrm) : 0.0;
-                column_update_kernel<P><<<blocks, kSpecThreads, 0, s>>>(X, n, k, Coef<P>{}, inv);
+                column_update_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(X, n, k, Coef<P>{}, inv);
                 MGB_LAUNCH_CHECK();
             }
     }
@@ -306,9 +310,9 @@ struct Solver {
         symmetric_eigen(H, P, theta, V);
         Coef<P> v{};
         for (int q = 0; q < P * P; ++q) v.v[q] = V[q];
-        rotate_kernel<P><<<blocks, kSpecThreads, 0, s>>>(X, n, v);
+        rotate_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(X, n, v);
         MGB_LAUNCH_CHECK();
-        rotate_kernel<P><<<blocks, kSpecThreads, 0, s>>>(Z, n, v);
+        rotate_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(Z, n, v);
         MGB_LAUNCH_CHECK();
         Coef<P> th{};
         for (int c = 0; c < P; ++c) th.v[c] = theta[c];
@@ -332,7 +336,7 @@ struct Solver {
         double* Z = static_cast<double*>(w.Z.ensure(sizeof(double) * (size_t)cnt));
         double* Y = static_cast<double*>(w.Y.ensure(sizeof(double) * (size_t)cnt));
         double* Yn = static_cast<double*>(w.Ynew.ensure(sizeof(double) * (size_t)cnt));
-        const int eb = spec_blocks(cnt);
+        const int eb = row_blocks(cnt);
         widen_kernel<<<eb, kSpecThreads, 0, s>>>(Xout, X, cnt);
         MGB_LAUNCH_CHECK();
         deflate(X);
@@ -392,12 +396,13 @@ void run_solver(const int32_t* indptr, const int32_t* indices, const float* data
     sv.indptr = indptr; sv.indices = indices; sv.data = data; sv.sd = sd; sv.comp = comp;
     sv.n = n; sv.n_comp = n_comp; sv.s = s;
     sv.blocks = spec_blocks(n);
+    sv.rblocks = row_blocks(n);
     sv.proj = static_cast<double*>(w.proj.ensure(sizeof(double) * (size_t)n_comp * P));
     double* tn = static_cast<double*>(w.tnorm.ensure(sizeof(double) * (size_t)n_comp));
     sv.part = static_cast<double*>(w.part.ensure(sizeof(double) * (size_t)sv.blocks * P * P));
     // tnorm[c] = sum over the component of t_i^2
     MGB_CUDA(cudaMemsetAsync(tn, 0, sizeof(double) * (size_t)n_comp, s));
-    component_sum_kernel<1><<<sv.blocks, kSpecThreads, 0, s>>>(sd, comp, n, nullptr, true, tn);
+    component_sum_kernel<1><<<sv.rblocks, kSpecThreads, 0, s>>>(sd, comp, n, nullptr, true, tn);
     MGB_LAUNCH_CHECK();
     sv.tnorm = tn;
     sv.run(X, n_wanted, degree, max_iter, tol, w);
