@@ -220,6 +220,16 @@ int mg_chebyshev_eigenvectors(const int32_t* indptr, const int32_t* indices, con
                               int64_t nnz, float* X, int p, const float* inv_sqrt_deg, const int32_t* component,
                               int n_wanted, int degree, int max_iter, float tol);
 
+/* The edge schedule of a fit, MAGNET._edge_schedule (magnet/__init__.py:726-737, with _sampling_frequencies of
+ * magnet/__init__.py:51-66), on the device: the CSR graph (indptr, indices, data) of n nodes -> the kept entries in
+ * CSR order as head (row), tail (column) and eps = 1 / freq, with freq = min(1, s w) summing to
+ * samples_per_node * n and kept when freq >= 1 / n_epochs; *n_kept their count. head, tail and eps hold nnz
+ * entries. s is solved in FP64 (bisection with block sums added in a fixed order, then exactly on its segment), so
+ * eps can differ from the host's sorted cumulative sum by FP64 rounding of s only. Host or device arrays. */
+int mg_edge_schedule(const int32_t* indptr, const int32_t* indices, const float* data, int64_t n, int64_t nnz,
+                     double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                     int64_t* n_kept);
+
 /* The edge schedule of MAGNET.transform (magnet/__init__.py:907-912, with _sampling_frequencies of
  * magnet/__init__.py:51-66), on the device: w (m, k) memberships of m new rows and ind (m, k) their neighbours
  * among n_train fixed rows -> the kept edges in row order, head[e] = n_train + row, tail[e] = ind, eps[e] = 1 / freq,

@@ -727,6 +727,31 @@ extern "C" int mg_chebyshev_eigenvectors(const int32_t* indptr, const int32_t* i
     });
 }
 
+extern "C" int mg_edge_schedule(const int32_t* indptr, const int32_t* indices, const float* data, int64_t n,
+                                int64_t nnz, double samples_per_node, int n_epochs, int32_t* head, int32_t* tail,
+                                float* eps, int64_t* n_kept) {
+    return guard([&] {
+        require(n >= 0 && nnz >= 0 && n_kept && (n == 0 || indptr), "need a CSR graph and n_kept");
+        require(nnz == 0 || (indices && data && head && tail && eps), "indices, data, head, tail and eps must hold nnz entries");
+        require(n_epochs >= 1 && samples_per_node > 0.0, "need n_epochs >= 1 and samples_per_node > 0");
+        require(n <= INT32_MAX, "node indices must fit 32 bits");
+        validate_csr_host(indptr, indices, nnz, n, -1, "edge_schedule");
+        cudaStream_t s = current_stream();
+        const int32_t* ip = in_dev(indptr, n + 1, 0, s);
+        const int32_t* ix = in_dev(indices, nnz, 1, s);
+        const float* w = in_dev(data, nnz, 2, s);
+        int32_t* hd = out_dev(head, nnz, 3);
+        int32_t* td = out_dev(tail, nnz, 4);
+        float* ed = out_dev(eps, nnz, 5);
+        const int64_t kept = edge_schedule_dev(ip, ix, w, n, nnz, samples_per_node, n_epochs, hd, td, ed, graph_work(), s);
+        back(head, hd, kept, s);
+        back(tail, td, kept, s);
+        back(eps, ed, kept, s);
+        MGB_CUDA(cudaStreamSynchronize(s));
+        *n_kept = kept;
+    });
+}
+
 extern "C" int mg_transform_schedule(const float* w, const int64_t* ind, int64_t m, int k, int64_t n_train,
                                      double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
                                      int64_t* n_kept) {

@@ -19,6 +19,7 @@
 #include "graph.cuh"
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 namespace mgb {
 
@@ -452,6 +453,66 @@ __global__ void __launch_bounds__(kSchedThreads) transform_schedule_kernel(
     if (threadIdx.x == 0) *n_kept = carry;
 }
 
+// ------------------------------------------------------------------------------------------------ fit schedule
+// block partials of the fit schedule's sums over the weights: mode 0: (sum w, count of w > 0, smallest positive
+// w); mode 1: (sum of min(1, s w), 0, 0); mode 2: (count of s w > 1, sum of the other w, 0)
+constexpr int kSchedBlocks = 4 * kNumSMs;
+
+__global__ void __launch_bounds__(kThreads) sched_sums_kernel(const float* __restrict__ w, int64_t n, int mode,
+                                                              double s, double* __restrict__ part) {
+    __shared__ double red[3][kThreads / 32];
+    double a = 0.0, b = 0.0, c = 1e300;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = (double)w[i];
+        if (mode == 0) { a += v; if (v > 0.0) { b += 1.0; c = fmin(c, v); } }
+        else if (mode == 1) a += fmin(1.0, s * v);
+        else if (s * v > 1.0) b += 1.0;
+        else a += v;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c = fmin(c, __shfl_xor_sync(0xffffffffu, c, o));
+    }
+    if (lane == 0) { red[0][warp] = a; red[1][warp] = b; red[2][warp] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0, tc = 1e300;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { ta += red[0][k]; tb += red[1][k]; tc = fmin(tc, red[2][k]); }
+        part[3 * blockIdx.x] = ta;
+        part[3 * blockIdx.x + 1] = tb;
+        part[3 * blockIdx.x + 2] = tc;
+    }
+}
+
+__device__ __forceinline__ double sched_freq(double v, double s, bool ones) { return ones ? 1.0 : fmin(1.0, s * v); }
+
+__global__ void sched_flag_kernel(const float* __restrict__ w, int64_t n, double s, bool ones, double min_freq,
+                                  int32_t* __restrict__ flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        flag[i] = sched_freq((double)w[i], s, ones) >= min_freq ? 1 : 0;
+}
+
+// one thread per row: its kept entries, in order, at their scanned offsets
+__global__ void sched_scatter_kernel(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                     const float* __restrict__ w, int64_t n_rows, double s, bool ones,
+                                     double min_freq, const int64_t* __restrict__ off, int32_t* __restrict__ head,
+                                     int32_t* __restrict__ tail, float* __restrict__ eps) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+        for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e) {
+            const double f = sched_freq((double)w[e], s, ones);
+            if (f >= min_freq) {
+                const int64_t pos = off[e];
+                head[pos] = (int32_t)r;
+                tail[pos] = indices[e];
+                eps[pos] = (float)(1.0 / f);
+            }
+        }
+    }
+}
+
 }  // namespace
 
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, DevBuf& tmp, cudaStream_t s) {
@@ -541,6 +602,67 @@ int64_t transform_schedule_dev(const float* w, const int64_t* ind, int64_t m, in
     MGB_LAUNCH_CHECK();
     int64_t kept = 0;
     MGB_CUDA(cudaMemcpyAsync(&kept, cnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    MGB_CUDA(cudaStreamSynchronize(s));
+    return kept;
+}
+
+namespace {
+// the three sums of sched_sums_kernel over the grid, its partials added on the host in block order
+void sched_sums(const float* w, int64_t n, int mode, double sc, GraphWork& gw, cudaStream_t s, double out[3]) {
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, kSchedBlocks));
+    double* part = static_cast<double*>(gw.s_part.ensure(sizeof(double) * 3 * kSchedBlocks));
+    sched_sums_kernel<<<blocks, kThreads, 0, s>>>(w, n, mode, sc, part);
+    MGB_LAUNCH_CHECK();
+    std::vector<double> h((size_t)3 * blocks);
+    MGB_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+    MGB_CUDA(cudaStreamSynchronize(s));
+    out[0] = 0.0; out[1] = 0.0; out[2] = 1e300;
+    for (int b = 0; b < blocks; ++b) {
+        out[0] += h[3 * b];
+        out[1] += h[3 * b + 1];
+        out[2] = std::min(out[2], h[3 * b + 2]);
+    }
+}
+}  // namespace
+
+int64_t edge_schedule_dev(const int32_t* indptr, const int32_t* indices, const float* w, int64_t n, int64_t nnz,
+                          double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                          GraphWork& gw, cudaStream_t s) {
+    if (nnz <= 0) return 0;
+    const double target = samples_per_node * (double)n;
+    double st[3];
+    sched_sums(w, nnz, 0, 0.0, gw, s, st);
+    const double sum = st[0], npos = st[1], wmin = st[2];
+    // the solution of _sampling_frequencies (magnet/__init__.py:51-66): all ones when nnz <= target; every
+    // positive weight saturated when they are too few (the reference's s = 1 / max(w_min, 1e-300)); else s exact
+    const bool ones = (double)nnz <= target;
+    double sc = 0.0;
+    if (!ones && npos <= target) {
+        sc = 1e300;
+    } else if (!ones) {
+        double lo = target / sum, hi = 1.0 / wmin;
+        for (int it = 0; it < 200 && hi > lo * (1.0 + 4e-16); ++it) {
+            const double mid = 0.5 * (lo + hi);
+            double f[3];
+            sched_sums(w, nnz, 1, mid, gw, s, f);
+            if (f[0] < target) lo = mid; else hi = mid;
+        }
+        double cr[3];
+        sched_sums(w, nnz, 2, lo, gw, s, cr);
+        sc = cr[0] > 0.0 ? (target - cr[1]) / cr[0] : hi;
+    }
+    const double min_freq = 1.0 / (double)n_epochs;
+    int32_t* flag = static_cast<int32_t*>(gw.s_flag.ensure(sizeof(int32_t) * (size_t)nnz));
+    int64_t* off = static_cast<int64_t*>(gw.s_off.ensure(sizeof(int64_t) * (size_t)(nnz + 1)));
+    const int eb = (int)std::max<int64_t>(1, std::min<int64_t>((nnz + kThreads - 1) / kThreads, 16 * kNumSMs));
+    sched_flag_kernel<<<eb, kThreads, 0, s>>>(w, nnz, sc, ones, min_freq, flag);
+    MGB_LAUNCH_CHECK();
+    exclusive_scan_i32(flag, nnz, off, gw.s_tmp, s);
+    const int rb = (int)std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, 16 * kNumSMs));
+    sched_scatter_kernel<<<rb, kThreads, 0, s>>>(indptr, indices, w, n, sc, ones, min_freq, off, head, tail, eps);
+    MGB_LAUNCH_CHECK();
+    int64_t kept = 0;
+    MGB_CUDA(cudaMemcpyAsync(&kept, off + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     MGB_CUDA(cudaStreamSynchronize(s));
     return kept;
 }

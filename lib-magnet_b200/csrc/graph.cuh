@@ -10,6 +10,7 @@ struct GraphWork {
     DevBuf sigma, rho, part, acol, aval, alen, tcnt, tptr, tcur, trow, tval, ucnt, uptr, scan, flag;
     DevBuf mid_state, mid_tab;   // mid-near partners: per-row stream states, jump tables and chunk tables
     DevBuf sched;                // the transform schedule's kept-edge count
+    DevBuf s_part, s_flag, s_off, s_tmp;   // the fit schedule's block partials, keep flags, offsets, scan tiles
 };
 
 // memberships (n_rows, k) of sorted neighbour distances; `target` = log2(n_neighbors) * bandwidth, computed by the
@@ -35,6 +36,14 @@ void mid_near_pairs_dev(const float* X, int64_t n, int d, int n_pairs, int n_can
 int64_t transform_schedule_dev(const float* w, const int64_t* ind, int64_t m, int k, int64_t n_train,
                                double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
                                GraphWork& gw, cudaStream_t s);
+// The edge schedule of a fit (MAGNET._edge_schedule, magnet/__init__.py:726-737) for the CSR graph (indptr, indices,
+// data) of n nodes: freq = min(1, s w) over the nnz entries, summing to samples_per_node * n, the entries with
+// freq >= 1 / n_epochs kept in CSR order as (head = row, tail = column, eps = 1 / freq) into arrays of nnz entries.
+// s is bracketed by bisection with block-partial sums added on the host in block order (the same bits every call),
+// then solved exactly on its segment. Returns the number kept (synchronises s).
+int64_t edge_schedule_dev(const int32_t* indptr, const int32_t* indices, const float* w, int64_t n, int64_t nnz,
+                          double samples_per_node, int n_epochs, int32_t* head, int32_t* tail, float* eps,
+                          GraphWork& gw, cudaStream_t s);
 // out[0..n] = exclusive scan of in[0..n) and, in out[n], the total (tmp: tile sums)
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, DevBuf& tmp, cudaStream_t s);
 // knn_search (src/nndescent.cpp:585-690): the beam search of queries Q (m, d) over the training rows X (n, d) and

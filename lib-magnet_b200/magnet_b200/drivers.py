@@ -234,14 +234,20 @@ def sampling_frequencies(w, target):
     return np.minimum(1.0, s * w)
 
 
-def edge_schedule(P, n_epochs, samples_per_node=5.0):
+def edge_schedule(P, n_epochs, samples_per_node=5.0, device=False):
     """Edges sampled every 1 / min(1, s w_i) epochs, s giving samples_per_node * n samples per epoch; edges visited
     less than once dropped (magnet/__init__.py:727-737). Returns (head, tail, epochs_per_sample) in the COO order
-    of the CSR (sorted by head)."""
+    of the CSR (sorted by head). device=True solves s on the device (mg_edge_schedule): the same edges, eps equal
+    up to FP64 rounding of s; the host path is the reference's arithmetic bit for bit."""
+    budget = n_epochs if isinstance(n_epochs, (int, np.integer)) else 300
+    if device:
+        from . import _native as N
+        P = sp.csr_matrix(P)
+        return N.edge_schedule_device(P.indptr.astype(np.int32), P.indices.astype(np.int32),
+                                      P.data.astype(np.float32), int(budget), float(samples_per_node))
     C = sp.csr_matrix(P).tocoo()
     w = C.data.astype(np.float64)
     freq = sampling_frequencies(w, samples_per_node * P.shape[0])
-    budget = n_epochs if isinstance(n_epochs, (int, np.integer)) else 300
     keep = freq >= 1.0 / budget
     return C.row[keep].astype(np.int32), C.col[keep].astype(np.int32), (1.0 / freq[keep]).astype(np.float32)
 

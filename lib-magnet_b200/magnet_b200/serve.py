@@ -351,7 +351,7 @@ def fit_layout(X, *, n_neighbors=15, n_epochs=200, a=None, b=None, seed=0, paral
     X = np.ascontiguousarray(X, dtype=np.float32)
     ind, dist = G.exact_knn(X, n_neighbors)
     P = G.fuzzy_graph(ind, dist, n_neighbors)
-    head, tail, eps = D.edge_schedule(P, n_epochs)
+    head, tail, eps = D.edge_schedule(P, n_epochs, device=True)
     Y = G.initial_layout(G.pca2(X, seed), seed)
     pairs = G.mid_near_pairs(X, 5, 6, seed=seed)
     D.optimize_sgd(Y, head, tail, eps, n_epochs, a=a, b=b, mid_weight=0.1, mid_pairs=pairs, graph=P, seed=seed,

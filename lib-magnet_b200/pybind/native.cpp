@@ -276,6 +276,26 @@ py::tuple knn_search(py::object X, py::object gptr, py::object gidx, py::object 
     return py::make_tuple(oi, od);
 }
 
+// MAGNET._edge_schedule (magnet/__init__.py:726-737) on the device: (head, tail, eps) of the kept entries of the
+// CSR graph, in CSR order, as host arrays
+py::tuple edge_schedule_device(py::object indptr, py::object indices, py::object data, int n_epochs,
+                               double samples_per_node) {
+    auto ip = view<int32_t>(indptr), ix = view<int32_t>(indices);
+    auto pd = view<float>(data);
+    if (ip.ndim() != 1 || ip.size() < 1) throw std::runtime_error("indptr must have n + 1 entries");
+    if (ix.size() != pd.size()) throw std::runtime_error("indices and data must have the same length");
+    const int64_t n = ip.size() - 1, nnz = ix.size();
+    py::array_t<int32_t> head(std::max<int64_t>(nnz, 1)), tail(std::max<int64_t>(nnz, 1));
+    py::array_t<float> eps(std::max<int64_t>(nnz, 1));
+    int64_t kept = 0;
+    {
+        py::gil_scoped_release rel;
+        check(mg_edge_schedule(ip.ptr, ix.ptr, pd.ptr, n, nnz, samples_per_node, n_epochs, head.mutable_data(),
+                               tail.mutable_data(), eps.mutable_data(), &kept));
+    }
+    return py::make_tuple(head[py::slice(0, kept, 1)], tail[py::slice(0, kept, 1)], eps[py::slice(0, kept, 1)]);
+}
+
 // chebyshev_eigenvectors (src/spectral.cpp:141-241) on the device; X is updated in place and returned, as the
 // reference returns its X argument
 py::object chebyshev_eigenvectors(py::object indptr, py::object indices, py::object data, py::object X,
@@ -421,6 +441,10 @@ PYBIND11_MODULE(_native, m) {
     m.def("knn_search", &knn_search, "Beam search of queries over a neighbour graph (dense data, device)",
           py::arg("X"), py::arg("gptr"), py::arg("gidx"), py::arg("landmarks"), py::arg("Q"), py::arg("k"),
           py::arg("ef") = 64, py::arg("n_entry") = 10, py::arg("seed") = 0, py::arg("n_threads") = -1);
+    m.def("edge_schedule_device", &edge_schedule_device,
+          "the edge schedule of a fit on the device: (head, tail, epochs_per_sample) of the kept CSR entries",
+          py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("n_epochs"),
+          py::arg("samples_per_node") = 5.0);
     m.def("chebyshev_eigenvectors", &chebyshev_eigenvectors,
           "Chebyshev-filtered subspace iteration for the leading non-trivial eigenvectors (device)",
           py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("X"), py::arg("inv_sqrt_deg"),

@@ -123,3 +123,19 @@ def test_chebyshev_argument_errors_without_gpu():
     assert rc == 1 and b"n_wanted + 1 columns" in lib.mg_last_error()
     rc = lib.mg_chebyshev_eigenvectors(None, None, None, 4, 0, X.ctypes.data, 3, None, None, 2, 1, 5, 0.05)
     assert rc == 1 and b"degree must be >= 2" in lib.mg_last_error()
+
+
+def test_edge_schedule_argument_errors_without_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(LIB)
+    lib.mg_last_error.restype = ctypes.c_char_p
+    P, I64 = ctypes.c_void_p, ctypes.c_int64
+    lib.mg_edge_schedule.argtypes = [P, P, P, I64, I64, ctypes.c_double, ctypes.c_int, P, P, P, ctypes.POINTER(I64)]
+    import numpy as np
+    ip = np.array([0, 1, 2], np.int32)
+    kept = I64(0)
+    rc = lib.mg_edge_schedule(ip.ctypes.data, None, None, 2, 2, 5.0, 100, None, None, None, ctypes.byref(kept))
+    assert rc == 1 and b"nnz entries" in lib.mg_last_error()
+    rc = lib.mg_edge_schedule(ip.ctypes.data, None, None, 2, 0, 5.0, 0, None, None, None, ctypes.byref(kept))
+    assert rc == 1 and b"n_epochs" in lib.mg_last_error()

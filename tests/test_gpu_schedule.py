@@ -71,3 +71,39 @@ def test_schedule_same_bits_every_call(mg):
     a = schedule_device(w, ind, 1000, 5.0, 100)
     b = schedule_device(w, ind, 1000, 5.0, 100)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def random_graph(n, deg, seed, zeros=0.0):
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n), deg)
+    cols = rng.integers(0, n, n * deg)
+    vals = (rng.random(n * deg) ** 3).astype(np.float32)
+    if zeros:
+        vals[rng.random(n * deg) < zeros] = 0.0
+    P = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    P.sum_duplicates()
+    return P
+
+
+@pytest.mark.parametrize("case", ["umap10k", "random", "zeros", "dense_target"])
+def test_fit_schedule_matches_host(mg, golden, case):
+    """MAGNET._edge_schedule (magnet/__init__.py:726-737) on the device against the host restatement pinned to the
+    reference's Python: the same kept entries in CSR order, eps equal in float32 up to one ulp"""
+    import scipy.sparse as sp
+    from magnet_b200 import drivers as D
+    if case == "umap10k":
+        g = golden("layout_config1.npz")
+        P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(len(g["indptr"]) - 1,) * 2)
+        epochs, spn = 500, 5.0
+    elif case == "random":
+        P, epochs, spn = random_graph(20000, 15, 1), 200, 5.0
+    elif case == "zeros":
+        P, epochs, spn = random_graph(5000, 12, 2, zeros=0.6), 200, 5.0
+    else:                                   # nnz <= samples_per_node * n: every frequency 1
+        P, epochs, spn = random_graph(3000, 4, 3), 200, 5.0
+    hh, th, eh = D.edge_schedule(P, epochs, spn)
+    hd, td, ed = D.edge_schedule(P, epochs, spn, device=True)
+    assert np.array_equal(hd, hh) and np.array_equal(td, th)
+    rel = np.abs(ed.astype(np.float64) - eh) / eh
+    assert rel.max() <= 1.2e-7 and np.mean(ed == eh) > 0.999, (rel.max(), np.mean(ed == eh))
