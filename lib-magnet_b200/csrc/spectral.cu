@@ -2,8 +2,8 @@
 // subspace iteration with Rayleigh-Ritz of the reference, in FP64 as the reference computes it. The block X is
 // n x p, row major (p <= 8 columns), as the reference holds it.
 //
-// Kernels: the SpMM of the lazy normalised adjacency (one thread per row, the row's entries in order, as
-// src/spectral.cpp:34-48); the deflation of the trivial eigenvector per connected component (per-component sums by
+// Kernels: the SpMM of the lazy normalised adjacency (a group of lanes per row, one per column, each summing the
+// row's entries in order, as src/spectral.cpp:34-48); the deflation of the trivial eigenvector per connected component (per-component sums by
 // block reductions and FP64 atomics); block-partial sums of the p x p products X^T B (Gram matrix, Rayleigh
 // quotient) and of the Ritz residuals, added on the host in block order; the filter's three-term recurrence, the
 // rotation by the Ritz vectors and the Gram-Schmidt updates as elementwise kernels. The small symmetric
@@ -29,28 +29,28 @@ int row_blocks(int64_t rows) {
 // the weight of node i on the trivial eigenvector: 1 / sd_i (0 for isolated nodes)
 __device__ __forceinline__ double trivial_of(float sd) { return sd > 0.f ? 1.0 / (double)sd : 0.0; }
 
-// out = M in, M = (I + D^-1/2 A D^-1/2) / 2 (src/spectral.cpp:34-48)
+// out = M in, M = (I + D^-1/2 A D^-1/2) / 2 (src/spectral.cpp:34-48): a group of G lanes per row (G the power of
+// two >= P), lane k summing column k over the row's entries in order, as the reference sums it; the group reads a
+// neighbour's P values as one contiguous run
 template <int P>
 __global__ void __launch_bounds__(kSpecThreads) spmm_kernel(const int32_t* __restrict__ indptr,
                                                             const int32_t* __restrict__ indices,
                                                             const float* __restrict__ data,
                                                             const float* __restrict__ sd, int64_t n,
                                                             const double* __restrict__ in, double* __restrict__ out) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double acc[P];
-#pragma unroll
-        for (int k = 0; k < P; ++k) acc[k] = 0.0;
+    constexpr int G = P <= 2 ? 2 : (P <= 4 ? 4 : 8);
+    const int k = threadIdx.x % G;
+    const int64_t groups = (int64_t)gridDim.x * (blockDim.x / G);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G; i < n; i += groups) {
+        double acc = 0.0;
         const int32_t e1 = indptr[i + 1];
+#pragma unroll 4
         for (int32_t j = indptr[i]; j < e1; ++j) {
             const int32_t col = indices[j];
             const double w = (double)data[j] * (double)sd[col];
-            const double* x = in + (int64_t)col * P;
-#pragma unroll
-            for (int k = 0; k < P; ++k) acc[k] += w * x[k];
+            if (k < P) acc += w * in[(int64_t)col * P + k];
         }
-        const double s = (double)sd[i];
-#pragma unroll
-        for (int k = 0; k < P; ++k) out[i * P + k] = 0.5 * (in[i * P + k] + s * acc[k]);
+        if (k < P) out[i * P + k] = 0.5 * (in[i * P + k] + (double)sd[i] * acc);
     }
 }
 
@@ -251,12 +251,12 @@ __global__ void narrow_kernel(const double* __restrict__ in, float* __restrict__
 template <int P>
 struct Solver {
     const int32_t* indptr; const int32_t* indices; const float* data; const float* sd; const int32_t* comp;
-    int64_t n; int n_comp; int blocks; int rblocks; cudaStream_t s;
+    int64_t n; int n_comp; int blocks; int rblocks; int sblocks; cudaStream_t s;
     double* proj; const double* tnorm; double* part;
     std::vector<double> host_part;
 
     void spmm(const double* in, double* out) {
-        spmm_kernel<P><<<rblocks, kSpecThreads, 0, s>>>(indptr, indices, data, sd, n, in, out);
+        spmm_kernel<P><<<sblocks, kSpecThreads, 0, s>>>(indptr, indices, data, sd, n, in, out);
         MGB_LAUNCH_CHECK();
     }
     void deflate(double* X) {
@@ -397,6 +397,7 @@ void run_solver(const int32_t* indptr, const int32_t* indices, const float* data
     sv.n = n; sv.n_comp = n_comp; sv.s = s;
     sv.blocks = spec_blocks(n);
     sv.rblocks = row_blocks(n);
+    sv.sblocks = row_blocks(n * (P <= 2 ? 2 : (P <= 4 ? 4 : 8)));   // a group of lanes per row
     sv.proj = static_cast<double*>(w.proj.ensure(sizeof(double) * (size_t)n_comp * P));
     double* tn = static_cast<double*>(w.tnorm.ensure(sizeof(double) * (size_t)n_comp));
     sv.part = static_cast<double*>(w.part.ensure(sizeof(double) * (size_t)sv.blocks * P * P));
