@@ -79,3 +79,18 @@ def test_wide_blocks_rejected(mg):
     a[3] = np.zeros((a[3].shape[0], 9), np.float32)
     with pytest.raises(RuntimeError, match="at most 8 columns"):
         N.chebyshev_eigenvectors(*a, -1)
+
+
+def test_one_wanted_vector_and_no_iterations(mg, ref, golden):
+    """n_wanted = 1 (a three-column block), and max_iter = 0 (the start block's Rayleigh-Ritz only)"""
+    if ref is None:
+        pytest.skip("reference module not built")
+    from magnet_b200 import _native as N
+    g = golden("layout_config1.npz")
+    P = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(len(g["indptr"]) - 1,) * 2)
+    compare(mg, ref, P, 1, seed=5)
+    a = list(inputs(P, 2, seed=6))
+    a[8] = 0
+    Xd = N.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1)
+    Xr = np.asarray(ref.chebyshev_eigenvectors(*a[:3], a[3].copy(), *a[4:], -1))
+    assert subspace_sine(Xd[:, :2], Xr[:, :2]) < 1e-6
